@@ -1,0 +1,336 @@
+#!/usr/bin/env python3
+"""Benchmark of the B200 wavefront spectral path tracer.
+
+Workload (a "step"): the uneven batch -- 64 renders drawn by seed from the 10
+Cornell scene variants, square resolutions log-uniform in 128..1024, depth
+2..8, paths per pixel log-uniform in 1..64, shadow rays 1..8, spectral
+hero-4, FP32 -- rendered by the batched method (one persistent wavefront
+over all 64 requests, graph-captured iterations).  Synthetic seeded data;
+the cornell-bunny variant uses a displaced icosphere of the bunny's size
+when the Stanford bunny OBJ is not present.
+
+Printed (rank 0, one JSON line):
+  value        batched paths/s (device time, CUDA events on the engine stream,
+               scene cache and requests resident; max over ranks for N > 1)
+  e2e          same metric through the C ABI with host buffers: submit from the
+               host, run, and copy every HDR + 8-bit image back, host clock
+  plain_value  the plain per-request method (one render per launch sequence)
+  roofline     dominant wavefront kernel vs measured HBM bandwidth
+  cpu_baseline the reference CPU renderer (oracle/_ref, built from the
+               reference sources) on a bounded row sample of the same batch
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "paths/s, batched+served wavefront (64 uneven spectral renders); plain per-request alongside"
+UNIT = "paths/s"
+HBM_FALLBACK = 6650.0
+
+
+def args_():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=3)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    p.add_argument("--renders", type=int, default=64)
+    p.add_argument("--seed", type=int, default=2026)
+    p.add_argument("--no-plain", action="store_true")
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-profile", action="store_true")
+    return p.parse_args()
+
+
+def peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return HBM_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                          "-i", str(self.device), "-lms", "200"], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) == 7:
+                try:
+                    rows.append([float(parts[0]), float(parts[1]), parts[2]] + parts[3:])
+                except ValueError:
+                    pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+                "samples": len(rows), "reasons": reasons}
+
+
+def make_batch(n, seed):
+    from pcr_b200 import workloads
+    return workloads.batch_requests(n, seed=seed)
+
+
+def scene_files():
+    from pcr_b200 import workloads
+    return {v: workloads.scene_path(v) for v in workloads.VARIANTS}, workloads.DEFAULT_DATA
+
+
+# ------------------------------------------------------------------ reference arm
+def cpu_sample_step(scenes, batch, rows):
+    """One bounded sample of the batch on the reference CPU renderer: `rows`
+    pixel rows of every request at its own depth / paths per pixel / shadow
+    rays (the reference's own castRaySpectral per path, samples = 1), all
+    host threads.  Returns (paths, seconds)."""
+    from oracle import ref
+    paths, secs = 0, 0.0
+    for r in batch:
+        o = ref.opts(r["width"], r["height"], depth=r["depth"], samples=1, shadow=r["shadow"], spectral=True,
+                     seed=r["seed"])
+        h = min(rows, r["height"])
+        _, s = ref.render_hdr(scenes[r["variant"]], o, mode=1, spp=r["samples"], threads=0, rows=(0, h))
+        paths += h * r["width"] * r["samples"]
+        secs += s
+    return paths, secs
+
+
+def reference_arm(a):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref
+    if not ref.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libpcrref.so not built"}))
+        return
+    files, data = scene_files()
+    scenes = {v: ref.load_scene(os.path.abspath(p), data) for v, p in files.items()}
+    batch = make_batch(a.renders, a.seed)
+    rows = 2
+    for _ in range(a.warmup):
+        cpu_sample_step(scenes, batch, rows)
+    tot_p, tot_s = 0, 0.0
+    for _ in range(a.steps):
+        p, s = cpu_sample_step(scenes, batch, rows)
+        tot_p += p
+        tot_s += s
+    v = tot_p / tot_s
+    cores = os.cpu_count()
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
+        "warmup": a.warmup, "ms_per_step": 1e3 * tot_s / a.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded batch of the 10 Cornell variants)",
+        "config": {"workload": f"batch{a.renders}-uneven", "sample": f"{rows} pixel rows of each render"},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{rows} rows of each of the {a.renders} renders per step"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ------------------------------------------------------------------ CUDA arm
+def main():
+    a = args_()
+    if a.impl == "reference":
+        reference_arm(a)
+        return
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import torch
+
+    from pcr_b200 import capi
+    torch.cuda.set_device(local)
+    ctx = capi.Context(device=local)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    files, data = scene_files()
+    sids = {v: ctx.load_scene_json(p, data) for v, p in files.items()}
+    batch = make_batch(a.renders, a.seed + rank)
+    descs = [capi.render_desc(r["width"], r["height"], depth=r["depth"], samples=r["samples"], shadow=r["shadow"],
+                              spectral=True, seed=r["seed"]) for r in batch]
+    step_paths = sum(r["width"] * r["height"] * r["samples"] for r in batch)
+
+    def batched_step(want_images=False):
+        ids = [ctx.submit(sids[r["variant"]], d) for r, d in zip(batch, descs)]
+        ctx.run_until_idle()
+        for i in ids:
+            ctx.fetch(i, want_hdr=want_images, want_rgb=want_images)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    for _ in range(a.warmup):
+        batched_step()
+    ctx.reset_stats()
+    # ---- device-timed batched region
+    barrier()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(local) as clk:
+        ev0.record(stream)
+        for _ in range(a.steps):
+            batched_step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    st = ctx.stats()
+    launches = sum(st["stage_launches"].values()) + a.steps * a.renders
+    total_paths = sum_over_ranks(step_paths * a.steps)
+    value = total_paths / (ms / 1e3)
+    rays = sum_over_ranks(st["rays"] + st["shadow_rays"]) / (ms / 1e3)
+
+    # ---- e2e: host buffers in and out through the C ABI, host clock
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(a.steps):
+        batched_step(want_images=True)
+    barrier()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = total_paths / e2e_s
+    d2h = sum(r["width"] * r["height"] * 15 for r in batch)
+    h2d = a.renders * 96
+
+    # ---- plain method on the same batch (one render per launch sequence)
+    plain = None
+    if not a.no_plain:
+        barrier()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for r, d in zip(batch, descs):
+            ctx.render(sids[r["variant"]], d, want_hdr=False, want_rgb=False)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        pms = max_over_ranks(p0.elapsed_time(p1))
+        plain = sum_over_ranks(step_paths) / (pms / 1e3)
+
+    # ---- per-stage events (profiled pass) for the roofline
+    roofline = None
+    if not a.no_profile:
+        pctx = capi.Context(device=local, profile=True)
+        psids = {v: pctx.load_scene_json(p, data) for v, p in files.items()}
+        ids = [pctx.submit(psids[r["variant"]], d) for r, d in zip(batch, descs)]
+        pctx.run_until_idle()
+        for i in ids:
+            pctx.fetch(i, want_hdr=False, want_rgb=False)
+        ps = pctx.stats()
+        pctx.close()
+        peak, kind = peaks()
+        # algorithmic bytes per unit (queue records, 16-byte words):
+        #   extend: ray in (origin, dir, id: 48 B) + hit out (16 B)
+        #   shadow: shadow record in (48 B)
+        #   shade : path in (64 B) + hit in (16 B) + path out (64 B) + shadow out (48 B each)
+        bytes_stage = {"extend": 64.0 * ps["rays"], "shadow": 48.0 * ps["shadow_rays"],
+                       "shade": 144.0 * ps["rays"] + 48.0 * ps["shadow_rays"]}
+        dom = max(bytes_stage, key=lambda k: ps["stage_ms"][k])
+        t_ms = ps["stage_ms"][dom]
+        n_l = max(1, ps["stage_launches"][dom])
+        achieved = bytes_stage[dom] / (t_ms / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                    "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                    "bytes_per_launch": bytes_stage[dom] / n_l, "ms_per_launch": t_ms / n_l,
+                    "stage_ms": ps["stage_ms"], "stage_share": {k: v / max(1e-9, sum(ps["stage_ms"].values()))
+                                                                for k, v in ps["stage_ms"].items()}}
+
+    # ---- CPU baseline (rank 0, N = 1): reference renderer on a row sample
+    cpu = None
+    if not a.no_cpu and rank == 0 and world == 1:
+        try:
+            from oracle import ref
+            if ref.available():
+                rscenes = {v: ref.load_scene(os.path.abspath(p), data) for v, p in files.items()}
+                pp, ss = cpu_sample_step(rscenes, batch, 2)
+                cpu = {"value": pp / ss, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                       "sample": f"2 pixel rows of each of the {a.renders} renders ({pp} paths, {ss:.1f} s)"}
+        except Exception as e:  # reported, not fatal
+            cpu = {"value": None, "error": str(e)}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
+            "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded 64-render batch of the 10 Cornell variants (bunny -> displaced icosphere "
+                    "stand-in when its OBJ is absent)",
+            "config": {"workload": f"batch{a.renders}-uneven", "renders": a.renders, "paths_per_step": step_paths,
+                       "resolution": "square, log-uniform 128..1024", "depth": "2..8", "paths_per_pixel": "1..64",
+                       "shadow_rays": "1..8", "spectral": "hero-4",
+                       "l2": "path/shadow queues ~2 GB > 126 MB L2 (no flush needed)"},
+            "rays_per_s": rays,
+            "plain_value": plain, "batched_over_plain": (value / plain) if plain else None,
+            "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+            "tuning": {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")},
+        }
+        print(json.dumps(out))
+    ctx.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

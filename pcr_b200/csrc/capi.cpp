@@ -1,0 +1,276 @@
+// extern "C" implementation of include/pcr_cuda.h.  No exception crosses
+// this boundary: every entry point converts errors into a pcr_status and a
+// thread-local message (pcr_last_error).
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "../../include/pcr_cuda.h"
+#include "engine.h"
+#include "scene.h"
+
+struct pcr_ctx {
+    std::unique_ptr<pcr::Engine> eng;
+};
+
+struct pcr_host_scene {
+    pcr::HostScene s;
+};
+
+namespace {
+thread_local std::string g_err;
+
+template <typename F>
+pcr_status guard(F&& f)
+{
+    try {
+        f();
+        g_err.clear();
+        return PCR_OK;
+    } catch (const pcr::PcrError& e) {
+        g_err = e.what();
+        return e.status;
+    } catch (const std::bad_alloc&) {
+        g_err = "host allocation failed";
+        return PCR_ERR_NO_MEMORY;
+    } catch (const std::exception& e) {
+        g_err = e.what();
+        return PCR_ERR_INVALID;
+    }
+}
+
+pcr::Engine& E(pcr_ctx* c)
+{
+    if (!c || !c->eng) throw pcr::PcrError(PCR_ERR_INVALID, "null context");
+    return *c->eng;
+}
+
+std::string parent_dir(const std::string& p)
+{
+    auto k = p.find_last_of('/');
+    return k == std::string::npos ? std::string(".") : (k == 0 ? std::string("/") : p.substr(0, k));
+}
+}  // namespace
+
+extern "C" {
+
+const char* pcr_last_error(void) { return g_err.c_str(); }
+const char* pcr_version(void) { return "pcr-b200 0.1 (sm_100a)"; }
+
+pcr_status pcr_ctx_create(pcr_ctx** out, const pcr_ctx_opts* opts)
+{
+    return guard([&] {
+        if (!out) throw pcr::PcrError(PCR_ERR_INVALID, "null output pointer");
+        auto c = std::make_unique<pcr_ctx>();
+        c->eng = std::make_unique<pcr::Engine>(opts);
+        *out = c.release();
+    });
+}
+
+pcr_status pcr_ctx_destroy(pcr_ctx* ctx)
+{
+    return guard([&] { delete ctx; });
+}
+
+pcr_status pcr_ctx_set_device(pcr_ctx* ctx)
+{
+    return guard([&] {
+        if (cudaSetDevice(E(ctx).device()) != cudaSuccess) throw pcr::PcrError(PCR_ERR_CUDA, "cudaSetDevice failed");
+    });
+}
+
+pcr_status pcr_ctx_stream(pcr_ctx* ctx, void** stream)
+{
+    return guard([&] {
+        if (!stream) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *stream = (void*)E(ctx).stream();
+    });
+}
+
+pcr_status pcr_scene_upload(pcr_ctx* ctx, const pcr_scene_desc* desc, pcr_scene_id* out)
+{
+    return guard([&] {
+        if (!desc || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *out = E(ctx).upload_scene(*desc);
+    });
+}
+
+pcr_status pcr_scene_load_json(pcr_ctx* ctx, const char* path, const char* data_root, const char* lut_path,
+                               pcr_scene_id* out)
+{
+    return guard([&] {
+        if (!path || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        // default data root: the directory that holds the scene directory
+        // (the reference ships <root>/Scenes/*.json beside <root>/spd/)
+        std::string root = data_root ? std::string(data_root) : parent_dir(parent_dir(path));
+        std::vector<float> lut;
+        if (lut_path) {
+            std::string err;
+            if (!pcr::load_plut(lut_path, lut, &err)) throw pcr::PcrError(PCR_ERR_SCENE, std::string("loadLUT(") + lut_path + "): " + err);
+        }
+        pcr::HostScene s = pcr::load_scene_json(path, root, lut_path ? &lut : nullptr);
+        pcr_scene_desc d = s.desc();
+        *out = E(ctx).upload_scene(d);
+    });
+}
+
+pcr_status pcr_host_scene_load(const char* path, const char* data_root, const char* lut_path, pcr_host_scene** out,
+                               pcr_scene_desc* desc)
+{
+    return guard([&] {
+        if (!path || !out || !desc) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        std::string root = data_root ? std::string(data_root) : parent_dir(parent_dir(path));
+        std::vector<float> lut;
+        if (lut_path) {
+            std::string err;
+            if (!pcr::load_plut(lut_path, lut, &err)) throw pcr::PcrError(PCR_ERR_SCENE, std::string("loadLUT(") + lut_path + "): " + err);
+        }
+        auto h = std::make_unique<pcr_host_scene>();
+        h->s = pcr::load_scene_json(path, root, lut_path ? &lut : nullptr);
+        *desc = h->s.desc();
+        *out = h.release();
+    });
+}
+
+pcr_status pcr_host_scene_free(pcr_host_scene* scene)
+{
+    return guard([&] { delete scene; });
+}
+
+pcr_status pcr_fit_sigmoid(const float* rgb, int64_t n, const float* lut, float* out4)
+{
+    return guard([&] {
+        if (!rgb || !out4 || n < 0) throw pcr::PcrError(PCR_ERR_INVALID, "bad argument");
+        std::vector<float> L;
+        if (lut) L.assign(lut, lut + 3 * 16 * 16 * 16 * 3);
+        for (int64_t i = 0; i < n; i++) pcr::fit_sigmoid(rgb + i * 3, lut ? &L : nullptr, out4 + i * 4);
+    });
+}
+
+pcr_status pcr_lut_build(float* out)
+{
+    return guard([&] {
+        if (!out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        std::vector<float> L;
+        pcr::build_lut(L);
+        std::memcpy(out, L.data(), L.size() * sizeof(float));
+    });
+}
+
+pcr_status pcr_scene_release(pcr_ctx* ctx, pcr_scene_id id)
+{
+    return guard([&] { E(ctx).release_scene(id); });
+}
+
+pcr_status pcr_scene_bytes(pcr_ctx* ctx, pcr_scene_id id, int64_t* bytes)
+{
+    return guard([&] {
+        if (!bytes) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *bytes = E(ctx).scene_bytes(id);
+    });
+}
+
+pcr_status pcr_render(pcr_ctx* ctx, pcr_scene_id scene, const pcr_render_desc* desc, float* hdr_out, uint8_t* rgb8_out,
+                      pcr_render_stats* stats)
+{
+    return guard([&] {
+        if (!desc) throw pcr::PcrError(PCR_ERR_INVALID, "null render descriptor");
+        E(ctx).render_plain(scene, *desc, hdr_out, rgb8_out, stats);
+    });
+}
+
+pcr_status pcr_submit(pcr_ctx* ctx, pcr_scene_id scene, const pcr_render_desc* desc, pcr_request_id* out)
+{
+    return guard([&] {
+        if (!desc || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *out = E(ctx).submit(scene, *desc);
+    });
+}
+
+pcr_status pcr_run_until_idle(pcr_ctx* ctx)
+{
+    return guard([&] { E(ctx).run_until_idle(); });
+}
+
+pcr_status pcr_serve_start(pcr_ctx* ctx)
+{
+    return guard([&] { E(ctx).serve_start(); });
+}
+
+pcr_status pcr_serve_stop(pcr_ctx* ctx)
+{
+    return guard([&] { E(ctx).serve_stop(); });
+}
+
+pcr_status pcr_poll(pcr_ctx* ctx, pcr_request_id id, int32_t* done)
+{
+    return guard([&] {
+        if (!done) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *done = E(ctx).poll(id) ? 1 : 0;
+    });
+}
+
+pcr_status pcr_wait(pcr_ctx* ctx, pcr_request_id id, int64_t timeout_ms)
+{
+    return guard([&] { E(ctx).wait(id, timeout_ms); });
+}
+
+pcr_status pcr_fetch(pcr_ctx* ctx, pcr_request_id id, float* hdr_out, uint8_t* rgb8_out, pcr_render_stats* stats)
+{
+    return guard([&] { E(ctx).fetch(id, hdr_out, rgb8_out, stats); });
+}
+
+pcr_status pcr_cancel(pcr_ctx* ctx, pcr_request_id id)
+{
+    return guard([&] { E(ctx).cancel(id); });
+}
+
+pcr_status pcr_engine_stats_get(pcr_ctx* ctx, pcr_engine_stats* out)
+{
+    return guard([&] {
+        if (!out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        E(ctx).stats(out);
+    });
+}
+
+pcr_status pcr_engine_stats_reset(pcr_ctx* ctx)
+{
+    return guard([&] { E(ctx).reset_stats(); });
+}
+
+pcr_status pcr_autotune(pcr_ctx* ctx, const pcr_scene_id* scenes, const pcr_render_desc* descs, int32_t n,
+                        int32_t* chosen)
+{
+    return guard([&] {
+        if (!scenes || !descs || n <= 0) throw pcr::PcrError(PCR_ERR_INVALID, "autotune needs a sample workload");
+        E(ctx).autotune(scenes, descs, n, chosen);
+    });
+}
+
+pcr_status pcr_trace_closest(pcr_ctx* ctx, pcr_scene_id scene, const float* rays, int64_t n, int32_t* mat,
+                             int32_t* prim, float* t)
+{
+    return guard([&] {
+        if (!rays && n > 0) throw pcr::PcrError(PCR_ERR_INVALID, "null rays");
+        E(ctx).trace(scene, rays, n, mat, prim, t, 0, nullptr);
+    });
+}
+
+pcr_status pcr_trace_bvh(pcr_ctx* ctx, pcr_scene_id scene, const float* rays, int64_t n, int32_t* tri_id, float* t,
+                         int32_t* counts)
+{
+    return guard([&] {
+        if (!rays && n > 0) throw pcr::PcrError(PCR_ERR_INVALID, "null rays");
+        E(ctx).trace(scene, rays, n, nullptr, tri_id, t, 1, counts);
+    });
+}
+
+pcr_status pcr_eval_stage(pcr_ctx* ctx, int32_t what, const float* params, const float* in, int64_t n, float* out)
+{
+    return guard([&] {
+        if (!in || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        E(ctx).eval_stage(what, params, in, n, out);
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,359 @@
+// Device functions of the wavefront path tracer.
+//
+// Intersection arithmetic uses explicit round-to-nearest intrinsics
+// (__fmul_rn/__fadd_rn/__fsub_rn/__fdiv_rn/__fsqrt_rn), which nvcc never
+// fuses into FMA, so every hit test performs the reference's float
+// operations in the reference's order (x86-64 g++ -O2 issues no FMA).  That is
+// what makes hit primitive ids bit-exact against the reference BVH.  Shading
+// arithmetic is free to contract.
+#pragma once
+
+#include <cfloat>
+#include <cstdint>
+
+#include "layout.h"
+
+namespace pcr {
+
+// ----------------------------------------------------------------- exact ops
+namespace ex {
+__device__ __forceinline__ float mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ float3 sub3(float3 a, float3 b) { return make_float3(sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)); }
+__device__ __forceinline__ float3 add3(float3 a, float3 b) { return make_float3(add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)); }
+__device__ __forceinline__ float3 scale3(float3 a, float s) { return make_float3(mul(a.x, s), mul(a.y, s), mul(a.z, s)); }
+// Vec3f::dot (Vec3f.h:16-19): (a0*b0 + a1*b1) + a2*b2
+__device__ __forceinline__ float dot(float3 a, float3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+// Vec3f::cross (Vec3f.h:21-28)
+__device__ __forceinline__ float3 cross(float3 a, float3 b)
+{
+    return make_float3(sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
+                       sub(mul(a.x, b.y), mul(a.y, b.x)));
+}
+__device__ __forceinline__ float3 normalize(float3 a)
+{
+    float m = __fsqrt_rn(dot(a, a));
+    return make_float3(div(a.x, m), div(a.y, m), div(a.z, m));
+}
+}  // namespace ex
+
+__device__ __forceinline__ float3 xyz(float4 v) { return make_float3(v.x, v.y, v.z); }
+__device__ __forceinline__ float3 f3add(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 f3sub(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 f3mul(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float f3dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 f3neg(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+
+// ----------------------------------------------------------------- primitives
+// Sphere::intersect (code/Includes/Sphere.h:20-40)
+__device__ __forceinline__ bool sphere_hit(const DSphere& s, float3 o, float3 d, float& t0)
+{
+    using namespace ex;
+    float4 cr = s.c_r;
+    float3 cp = sub3(make_float3(cr.x, cr.y, cr.z), o);
+    float rayLen = dot(d, cp);
+    float tSq = sub(dot(cp, cp), mul(rayLen, rayLen));
+    float r2 = mul(cr.w, cr.w);
+    if (tSq > r2) return false;
+    float tDist = __fsqrt_rn(sub(r2, tSq));
+    t0 = sub(rayLen, tDist);
+    float t1 = add(rayLen, tDist);
+    if (t0 < 0) t0 = t1;
+    if (t0 < 0) return false;
+    return true;
+}
+
+// Plane::intersect (code/Includes/Plane.h:33-54); uu, vv precomputed with
+// the same dot the reference evaluates per call.
+__device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, float closest, float& t0)
+{
+    using namespace ex;
+    float4 nA = p.n_area;
+    float3 N = make_float3(nA.x, nA.y, nA.z);
+    float denom = dot(d, N);
+    if (fabsf(denom) <= 1e-6f) return false;
+    float4 oM = p.o_mat;
+    float3 po = make_float3(oM.x, oM.y, oM.z);
+    float t = div(dot(sub3(po, o), N), denom);
+    t0 = t;
+    if (t <= 1e-6f || t > closest) return false;
+    float3 lh = sub3(add3(o, scale3(d, t)), po);
+    float4 u = p.u_uu, v = p.v_vv;
+    float s = div(dot(lh, make_float3(u.x, u.y, u.z)), u.w);
+    float q = div(dot(lh, make_float3(v.x, v.y, v.z)), v.w);
+    if (s > 1.f || s < 0.f || q > 1.f || q < 0.f) return false;
+    return true;
+}
+
+// Triangle::intersect (code/Includes/Triangle.h:53-92), Moller-Trumbore.
+__device__ __forceinline__ bool tri_hit(float4 a, float4 b, float4 c, float3 o, float3 d, float closest,
+                                        float& t_out, float& u_out, float& v_out)
+{
+    using namespace ex;
+    float3 v0 = make_float3(a.x, a.y, a.z), e1 = make_float3(b.x, b.y, b.z), e2 = make_float3(c.x, c.y, c.z);
+    float3 pvec = cross(d, e2);
+    float det = dot(e1, pvec);
+    if (fabsf(det) < 1e-6f) return false;
+    float invDet = div(1.f, det);
+    float3 tvec = sub3(o, v0);
+    float u = mul(dot(tvec, pvec), invDet);
+    if (u < 0.f || u > 1.f) return false;
+    float3 qvec = cross(tvec, e1);
+    float v = mul(dot(d, qvec), invDet);
+    if (v < 0.f || add(u, v) > 1.f) return false;
+    float t = mul(dot(e2, qvec), invDet);
+    if (t <= 1e-6f || t >= closest) return false;
+    t_out = t;
+    u_out = u;
+    v_out = v;
+    return true;
+}
+
+// Slab test of one child box with the reference's arithmetic
+// (code/Bvh/Bvh.cpp:360-377); inv = 1/dir per axis, NaN lanes ignored the
+// way std::max/std::min ignore a NaN second argument.
+__device__ __forceinline__ bool slab(float lx, float hx, float ly, float hy, float lz, float hz, float3 o, float3 inv,
+                                     float segMax, float& tNear)
+{
+    using namespace ex;
+    float tmin = 0.f, tmax = segMax;
+    float t1 = mul(sub(lx, o.x), inv.x), t2 = mul(sub(hx, o.x), inv.x);
+    if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+    tmin = (tmin < t1) ? t1 : tmin;
+    tmax = (t2 < tmax) ? t2 : tmax;
+    if (tmin > tmax) return false;
+    t1 = mul(sub(ly, o.y), inv.y); t2 = mul(sub(hy, o.y), inv.y);
+    if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+    tmin = (tmin < t1) ? t1 : tmin;
+    tmax = (t2 < tmax) ? t2 : tmax;
+    if (tmin > tmax) return false;
+    t1 = mul(sub(lz, o.z), inv.z); t2 = mul(sub(hz, o.z), inv.z);
+    if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
+    tmin = (tmin < t1) ? t1 : tmin;
+    tmax = (t2 < tmax) ? t2 : tmax;
+    if (tmin > tmax) return false;
+    tNear = tmin;
+    return true;
+}
+
+struct TraceCounts { int nodes, tris; };
+
+// Closest hit over the 4-wide BVH (ordered traversal, stack in local memory).
+// `closest` comes in as the best t from spheres/planes.  Returns the leaf-order
+// triangle index or -1; t/u/v of the hit.
+template <bool kCount>
+__device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d, float& closest, float& hu, float& hv,
+                                            TraceCounts* cnt)
+{
+    if (S.n_nodes <= 0) return -1;
+    float3 inv = make_float3(__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdiv_rn(1.f, d.z));
+    int stk[kStackSize];
+    float stt[kStackSize];
+    int top = 0;
+    int best = -1;
+    stk[top] = 0; stt[top] = 0.f; top++;
+    while (top > 0) {
+        --top;
+        int code = stk[top];
+        if (stt[top] > closest) continue;
+        if (code >= 0) {
+            const DNode4* n = S.nodes + code;
+            float4 lx = __ldg(&n->lox), hx = __ldg(&n->hix), ly = __ldg(&n->loy), hy = __ldg(&n->hiy);
+            float4 lz = __ldg(&n->loz), hz = __ldg(&n->hiz);
+            int4 ch = __ldg(&n->child), va = __ldg(&n->valid);
+            if (kCount) cnt->nodes++;
+            float tn[4];
+            int cc[4];
+            int k = 0;
+            float t;
+            if (va.x && slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.x; k++; }
+            if (va.y && slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.y; k++; }
+            if (va.z && slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.z; k++; }
+            if (va.w && slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.w; k++; }
+            // push far-to-near so the nearest child pops first
+            for (int i = 1; i < k; i++) {
+                float kt = tn[i];
+                int kc = cc[i];
+                int j = i - 1;
+                while (j >= 0 && tn[j] < kt) { tn[j + 1] = tn[j]; cc[j + 1] = cc[j]; j--; }
+                tn[j + 1] = kt; cc[j + 1] = kc;
+            }
+            if (top + k > kStackSize) continue;  // mirrors the reference's overflow guard
+            for (int i = 0; i < k; i++) { stk[top] = cc[i]; stt[top] = tn[i]; top++; }
+        } else {
+            int first = code & 0x00FFFFFF;
+            int count = (code >> 24) & 0x7F;
+            for (int i = 0; i < count; i++) {
+                const DTri* tr = S.tris + first + i;
+                float4 a = __ldg(&tr->v0_id), b = __ldg(&tr->e1_mat), c = __ldg(&tr->e2_flags);
+                if (kCount) cnt->tris++;
+                float t, u, v;
+                if (tri_hit(a, b, c, o, d, closest, t, u, v)) {
+                    closest = t;
+                    hu = u;
+                    hv = v;
+                    best = first + i;
+                }
+            }
+        }
+    }
+    return best;
+}
+
+// Renderer::sceneIntersect (code/Renderer.cpp:891-949): spheres, then planes
+// (light planes first), then the triangle BVH; first-tested wins ties.
+// Returns the primitive code; t and barycentrics through refs.
+__device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, float3 d, float tmax, float& t, float& hu,
+                                                  float& hv)
+{
+    float closest = tmax;
+    uint32_t prim = kPrimNone;
+    for (int i = 0; i < S.n_spheres; i++) {
+        float t0;
+        if (sphere_hit(S.spheres[i], o, d, t0) && t0 < closest) {
+            closest = t0;
+            prim = kPrimSphere | (uint32_t)i;
+        }
+    }
+    for (int i = 0; i < S.n_planes; i++) {
+        float t0;
+        if (plane_hit(S.planes[i], o, d, closest, t0) && t0 < closest) {
+            closest = t0;
+            prim = kPrimPlane | (uint32_t)i;
+        }
+    }
+    int tri = bvh4_closest<false>(S, o, d, closest, hu, hv, nullptr);
+    if (tri >= 0) prim = kPrimTri | (uint32_t)tri;
+    t = closest;
+    return prim;
+}
+
+// ----------------------------------------------------------------- spectra
+// The stage functions below use the exact (never-contracted) ops: the
+// sigmoid 0.5 + p / (2 sqrt(1 + p^2)) cancels for strongly negative p, where
+// a fused multiply-add would move the result by more than 1e-5 relative.
+__device__ __forceinline__ float sigmoid_fit(float4 f, float lambda)
+{
+    // RGBToSpectrum::evalSigmoidFit (code/Includes/RGBToSpectrum.h:118-125)
+    using namespace ex;
+    float L = div(sub(lambda, 550.f), 150.f);
+    float p = add(f.x, mul(L, add(f.y, mul(L, f.z))));
+    return mul(add(0.5f, div(p, mul(2.f, __fsqrt_rn(add(1.f, mul(p, p)))))), f.w);
+}
+
+__device__ __forceinline__ float spectrum_lerp(const float* s, float lambda)
+{
+    // Spectrum::operator() (code/Includes/Spectrum.h:82-90)
+    using namespace ex;
+    if (lambda < 400.f || lambda > 700.f) return 0.f;
+    float t = div(sub(lambda, 400.f), 5.0f);
+    int i = (int)t;
+    if (i >= kSpecN - 1) return s[kSpecN - 1];
+    float f = sub(t, (float)i);
+    return add(mul(s[i], sub(1.f, f)), mul(s[i + 1], f));
+}
+
+// Material::albedoAt / emissiveAt (code/Includes/Material.h:92-101)
+__device__ __forceinline__ float albedo_at(const DMaterial& m, float lambda)
+{
+    if (m.flags & kMatTabA) return spectrum_lerp(m.tabA, lambda);
+    float v = sigmoid_fit(m.afit, lambda);
+    return v > 1.f ? 1.f : v;
+}
+__device__ __forceinline__ float emissive_at(const DMaterial& m, float lambda)
+{
+    if (m.flags & kMatTabE) return spectrum_lerp(m.tabE, lambda);
+    return sigmoid_fit(m.efit, lambda);
+}
+
+// Wyman-Sloan-Shirley piecewise Gaussians (code/Includes/CIE.h:27-53)
+__device__ __forceinline__ float wyman(float l, float mu, float s1, float s2)
+{
+    using namespace ex;
+    float t = (l < mu) ? mul(sub(l, mu), s1) : mul(sub(l, mu), s2);
+    return expf(mul(mul(-0.5f, t), t));
+}
+__device__ __forceinline__ float3 cmf(float l)
+{
+    using namespace ex;
+    float x = sub(add(mul(0.362f, wyman(l, 442.0f, 0.0624f, 0.0374f)), mul(1.056f, wyman(l, 599.8f, 0.0264f, 0.0323f))),
+                  mul(0.065f, wyman(l, 501.1f, 0.0490f, 0.0382f)));
+    float y = add(mul(0.821f, wyman(l, 568.8f, 0.0213f, 0.0247f)), mul(0.286f, wyman(l, 530.9f, 0.0613f, 0.0322f)));
+    float z = add(mul(1.217f, wyman(l, 437.0f, 0.0845f, 0.0278f)), mul(0.681f, wyman(l, 459.0f, 0.0385f, 0.0725f)));
+    return make_float3(x, y, z);
+}
+
+// XYZ -> linear sRGB, D65 (code/Includes/CIE.h:115-123)
+__device__ __forceinline__ float3 xyz_to_srgb(float3 c)
+{
+    using namespace ex;
+    return make_float3(sub(sub(mul(3.2404542f, c.x), mul(1.5371385f, c.y)), mul(0.4985314f, c.z)),
+                       add(add(mul(-0.9692660f, c.x), mul(1.8760108f, c.y)), mul(0.0415560f, c.z)),
+                       add(sub(mul(0.0556434f, c.x), mul(0.2040259f, c.y)), mul(1.0572252f, c.z)));
+}
+
+// ToneMap::reinhard / aces (code/Includes/ToneMap.h:14-39)
+__device__ __forceinline__ float reinhard(float x) { return __fdiv_rn(x, __fadd_rn(x, 1.f)); }
+__device__ __forceinline__ float aces(float x)
+{
+    using namespace ex;
+    float v = div(mul(x, add(mul(2.51f, x), 0.03f)), add(mul(x, add(mul(2.43f, x), 0.59f)), 0.14f));
+    return v < 0.f ? 0.f : (v > 1.f ? 1.f : v);
+}
+// (unsigned char)(255*c + 0.5f) as x86-64 lowers it: truncate to int32, keep
+// the low byte (code/Renderer.cpp:379-381).
+__device__ __forceinline__ unsigned char quantize(float c)
+{
+    float v = __fadd_rn(__fmul_rn(255.f, c), 0.5f);
+    if (!(v > -2147483648.0f && v < 2147483648.0f)) return 0;
+    return (unsigned char)(__float2int_rz(v) & 0xFF);
+}
+
+// ----------------------------------------------------------------- RNG
+// Counter-based: pcg4d (Jarzynski & Olano, "Hash Functions for GPU
+// Rendering", JCGT 2020) keyed on (pixel, sample|fork, seed^bounce, seed^dim).
+// A path's random numbers depend only on its request seed, pixel, sample,
+// fork channel, bounce and dimension, never on its queue slot, so a render
+// is the same alone or batched with others.
+__device__ __forceinline__ uint4 pcg4d(uint4 v)
+{
+    v.x = v.x * 1664525u + 1013904223u;
+    v.y = v.y * 1664525u + 1013904223u;
+    v.z = v.z * 1664525u + 1013904223u;
+    v.w = v.w * 1664525u + 1013904223u;
+    v.x += v.y * v.w; v.y += v.z * v.x; v.z += v.x * v.y; v.w += v.y * v.z;
+    v.x ^= v.x >> 16; v.y ^= v.y >> 16; v.z ^= v.z >> 16; v.w ^= v.w >> 16;
+    v.x += v.y * v.w; v.y += v.z * v.x; v.z += v.x * v.y; v.w += v.y * v.z;
+    return v;
+}
+__device__ __forceinline__ float u01(uint32_t x) { return (float)(x >> 8) * (1.0f / 16777216.0f); }
+__device__ __forceinline__ float4 rand4(const DRequest& R, uint32_t pixel, uint32_t sample, uint32_t fork, uint32_t bounce,
+                                        uint32_t dim)
+{
+    uint4 v = make_uint4(pixel, sample ^ (fork << 27), R.seed_lo ^ (bounce * 0x9E3779B9u),
+                         R.seed_hi + dim * 0x85EBCA6Bu);
+    v = pcg4d(v);
+    return make_float4(u01(v.x), u01(v.y), u01(v.z), u01(v.w));
+}
+
+// Cosine hemisphere (code/Includes/Ray.h:37-53): disk sample, helper axis,
+// T = normalize(N x helper), B = N x T.  The direction is not renormalised.
+__device__ __forceinline__ float3 hemisphere(float3 N, float r1, float r2)
+{
+    float3 helper = fabsf(N.x) <= fabsf(N.y) ? make_float3(1.f, 0.f, 0.f) : make_float3(0.f, 1.f, 0.f);
+    float3 T = make_float3(N.y * helper.z - N.z * helper.y, N.z * helper.x - N.x * helper.z,
+                           N.x * helper.y - N.y * helper.x);
+    float tl = rsqrtf(f3dot(T, T));
+    T = f3mul(T, tl);
+    float3 B = make_float3(N.y * T.z - N.z * T.y, N.z * T.x - N.x * T.z, N.x * T.y - N.y * T.x);
+    float r = sqrtf(r1);
+    float s, c;
+    sincospif(2.f * r2, &s, &c);
+    float x = r * c, y = r * s;
+    float z = sqrtf(fmaxf(0.f, 1.f - x * x - y * y));
+    return make_float3(T.x * x + B.x * y + N.x * z, T.y * x + B.y * y + N.y * z, T.z * x + B.z * y + N.z * z);
+}
+
+}  // namespace pcr

@@ -1,0 +1,1115 @@
+// Host side of the wavefront engine.  See engine.h.
+#include "engine.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "kernels.cuh"
+#include "scene.h"
+
+namespace pcr {
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess)                                                                     \
+            throw PcrError(e_ == cudaErrorMemoryAllocation ? PCR_ERR_NO_MEMORY : PCR_ERR_CUDA,     \
+                           std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+// ---------------------------------------------------------------- small setter kernels
+// Request entries and the active list travel as kernel parameters, which
+// the launch copies, so the host never races an in-flight copy.
+struct ActiveList { int n; int slots[kMaxActive]; };
+
+__global__ void k_admit(EngineView E, DRequest r, int slot)
+{
+    const_cast<DRequest*>(E.reqs)[slot] = r;
+    E.issued[slot] = 0ull;
+    E.outstanding[slot] = 0;
+    E.done_flag[slot] = 0;
+    E.t_first[slot] = 0ull;
+    E.t_done[slot] = 0ull;
+}
+
+__global__ void k_set_active(EngineView E, ActiveList L)
+{
+    for (int i = threadIdx.x; i < L.n; i += blockDim.x) E.active[i] = L.slots[i];
+    if (threadIdx.x == 0) *E.n_active = L.n;
+}
+
+__global__ void k_set_params(EngineParams* P, EngineParams p) { *P = p; }
+
+// ---------------------------------------------------------------- helpers
+static float host_ybar_integral()
+{
+    // CIE::yBarIntegral (code/Includes/CIE.h:79-88), float arithmetic in the
+    // reference's order (this file's host code is built without FMA contraction).
+    auto wy = [](float l, float mu, float s1, float s2) {
+        float t = (l < mu) ? (l - mu) * s1 : (l - mu) * s2;
+        return std::exp(-0.5f * t * t);
+    };
+    float sum = 0.f;
+    for (int i = 0; i < kSpecN; i++) {
+        float l = 400.f + i * 5.0f;
+        sum += 0.821f * wy(l, 568.8f, 0.0213f, 0.0247f) + 0.286f * wy(l, 530.9f, 0.0613f, 0.0322f);
+    }
+    return sum * 5.0f;
+}
+
+template <typename T>
+static T* dalloc(size_t n, std::vector<void*>& track)
+{
+    T* p = nullptr;
+    if (n == 0) n = 1;
+    CK(cudaMalloc(&p, n * sizeof(T)));
+    track.push_back(p);
+    return p;
+}
+
+template <typename T>
+static T* dupload(const std::vector<T>& v, std::vector<void*>& track, int64_t& bytes)
+{
+    T* p = dalloc<T>(v.size(), track);
+    if (!v.empty()) CK(cudaMemcpy(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice));
+    bytes += (int64_t)std::max<size_t>(1, v.size()) * sizeof(T);
+    return p;
+}
+
+// ---------------------------------------------------------------- ctor / dtor
+Engine::Engine(const pcr_ctx_opts* o)
+{
+    if (o) {
+        device_ = o->device;
+        if (o->memory_budget > 0) budget_ = o->memory_budget;
+        if (o->queue_capacity > 0) tune_.queue_capacity = o->queue_capacity;
+        if (o->block_size > 0) tune_.block_size = o->block_size;
+        if (o->chunk_paths > 0) tune_.chunk_paths = o->chunk_paths;
+        if (o->regen_every > 0) tune_.regen_every = o->regen_every;
+        use_graph_ = o->use_graph != 0;
+        profile_ = o->profile != 0;
+        if (o->tuning_cache) tuning_cache_ = o->tuning_cache;
+    }
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (ndev <= 0) throw PcrError(PCR_ERR_CUDA, "no CUDA device");
+    if (device_ < 0 || device_ >= ndev) throw PcrError(PCR_ERR_INVALID, "device ordinal out of range");
+    CK(cudaSetDevice(device_));
+    CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
+    CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    xyz_scale_ = (700.f - 400.f) / host_ybar_integral();
+    slot_owner_.assign(kMaxActive, -1);
+    scenes_.reserve(256);
+    for (auto& e : prof_ev_) CK(cudaEventCreate(&e));
+    CK(cudaEventCreateWithFlags(&ev_snap_, cudaEventDisableTiming));
+    alloc_buffers();
+}
+
+Engine::~Engine()
+{
+    try {
+        serve_stop();
+    } catch (...) {
+    }
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(stream_);
+    for (auto& kv : reqs_) {
+        Request& r = *kv.second;
+        if (r.accum) cudaFree(r.accum);
+        if (r.d_hdr) cudaFree(r.d_hdr);
+        if (r.d_rgb) cudaFree(r.d_rgb);
+        if (r.h_hdr) cudaFreeHost(r.h_hdr);
+        if (r.h_rgb) cudaFreeHost(r.h_rgb);
+        if (r.ev_ready) cudaEventDestroy(r.ev_ready);
+    }
+    for (auto& s : scenes_)
+        for (void* p : s.allocs) cudaFree(p);
+    free_buffers();
+    for (auto& e : prof_ev_) cudaEventDestroy(e);
+    cudaEventDestroy(ev_snap_);
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    cudaStreamDestroy(stream_);
+}
+
+void Engine::alloc_buffers()
+{
+    std::vector<void*>& T = qallocs_;
+    d_scenes_ = dalloc<DScene>(256, T);
+    mat_cap_ = 256;
+    d_mats_ = dalloc<DMaterial>(mat_cap_, T);
+    d_reqs_ = dalloc<DRequest>(kMaxActive, T);
+    CK(cudaMemset(d_reqs_, 0, sizeof(DRequest) * kMaxActive));
+    d_issued_ = dalloc<unsigned long long>(kMaxActive, T);
+    d_tfirst_ = dalloc<unsigned long long>(kMaxActive, T);
+    d_tdone_ = dalloc<unsigned long long>(kMaxActive, T);
+    d_outstanding_ = dalloc<long long>(kMaxActive, T);
+    d_give_start_ = dalloc<long long>(kMaxActive, T);
+    d_give_ = dalloc<int>(kMaxActive, T);
+    d_give_base_ = dalloc<int>(kMaxActive, T);
+    d_active_ = dalloc<int>(kMaxActive, T);
+    d_nactive_ = dalloc<int>(1, T);
+    d_done_ = dalloc<int>(kMaxActive, T);
+    d_cnt_ = dalloc<Counters>(1, T);
+    d_params_ = dalloc<EngineParams>(1, T);
+    CK(cudaMemset(d_issued_, 0, 8 * kMaxActive));
+    CK(cudaMemset(d_outstanding_, 0, 8 * kMaxActive));
+    CK(cudaMemset(d_done_, 0, 4 * kMaxActive));
+    CK(cudaMemset(d_nactive_, 0, 4));
+    CK(cudaMemset(d_cnt_, 0, sizeof(Counters)));
+    CK(cudaMallocHost(&h_snap_, sizeof(HostSnap)));
+    CK(cudaMallocHost(&h_params_, sizeof(EngineParams)));
+
+    const int fill = tune_.queue_capacity;
+    queue_cap_ = fill * 4;   // a dispersive-glass fork turns one path into up to four
+    shadow_cap_ = (int)std::min<int64_t>((int64_t)queue_cap_ * 8, (1ll << 31) - 1);
+    for (int b = 0; b < 2; b++) {
+        q_[b].o = dalloc<float4>(queue_cap_, T);
+        q_[b].d = dalloc<float4>(queue_cap_, T);
+        q_[b].tp = dalloc<float4>(queue_cap_, T);
+        q_[b].id = dalloc<int4>(queue_cap_, T);
+    }
+    d_hit_ = dalloc<float4>(queue_cap_, T);
+    sq_.o = dalloc<float4>(shadow_cap_, T);
+    sq_.d = dalloc<float4>(shadow_cap_, T);
+    sq_.c = dalloc<float4>(shadow_cap_, T);
+    EngineParams p{fill, tune_.chunk_paths, tune_.regen_every, 0};
+    CK(cudaMemcpy(d_params_, &p, sizeof(p), cudaMemcpyHostToDevice));
+    graph_dirty_ = true;
+}
+
+void Engine::free_buffers()
+{
+    for (void* p : qallocs_) cudaFree(p);
+    qallocs_.clear();
+    if (h_snap_) cudaFreeHost(h_snap_);
+    if (h_params_) cudaFreeHost(h_params_);
+    h_snap_ = nullptr;
+    h_params_ = nullptr;
+}
+
+void Engine::set_tuning(const EngineTuning& t)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    for (int s : active_slots_)
+        if (s >= 0) throw PcrError(PCR_ERR_INVALID, "cannot retune while requests are active");
+    CK(cudaStreamSynchronize(stream_));
+    // keep the scene and material tables; rebuild queues and the request table
+    std::vector<DScene> sc(256);
+    CK(cudaMemcpy(sc.data(), d_scenes_, sizeof(DScene) * 256, cudaMemcpyDeviceToHost));
+    std::vector<DMaterial> mats(mat_count_);
+    if (mat_count_) CK(cudaMemcpy(mats.data(), d_mats_, sizeof(DMaterial) * mat_count_, cudaMemcpyDeviceToHost));
+    free_buffers();
+    tune_ = t;
+    if (tune_.iters_per_launch < 2) tune_.iters_per_launch = 2;
+    if (tune_.iters_per_launch & 1) tune_.iters_per_launch++;
+    alloc_buffers();
+    if (mat_count_ > mat_cap_) {
+        mat_cap_ = mat_count_;
+    }
+    CK(cudaMemcpy(d_scenes_, sc.data(), sizeof(DScene) * 256, cudaMemcpyHostToDevice));
+    if (mat_count_) {
+        if (mat_count_ > 256) {
+            CK(cudaFree(d_mats_));
+            qallocs_.erase(std::find(qallocs_.begin(), qallocs_.end(), (void*)d_mats_));
+            d_mats_ = dalloc<DMaterial>(mat_cap_, qallocs_);
+        }
+        CK(cudaMemcpy(d_mats_, mats.data(), sizeof(DMaterial) * mat_count_, cudaMemcpyHostToDevice));
+    }
+    if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    graph_exec_ = nullptr;
+    graph_dirty_ = true;
+}
+
+EngineView Engine::view() const
+{
+    EngineView E{};
+    E.scenes = d_scenes_;
+    E.mats = d_mats_;
+    E.reqs = d_reqs_;
+    E.issued = d_issued_;
+    E.outstanding = d_outstanding_;
+    E.give = d_give_;
+    E.give_base = d_give_base_;
+    E.active = d_active_;
+    E.n_active = d_nactive_;
+    E.done_flag = d_done_;
+    E.t_first = d_tfirst_;
+    E.t_done = d_tdone_;
+    E.cnt = d_cnt_;
+    E.q[0] = q_[0];
+    E.q[1] = q_[1];
+    E.hit = d_hit_;
+    E.sq = sq_;
+    E.give_start = d_give_start_;
+    E.shadow_cap = shadow_cap_;
+    E.queue_cap = queue_cap_;
+    E.n_mats = mat_count_;
+    return E;
+}
+
+// ---------------------------------------------------------------- scenes
+int Engine::upload_scene(const pcr_scene_desc& d)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    if (d.n_materials <= 0 || !d.materials) throw PcrError(PCR_ERR_INVALID, "scene has no materials");
+    if (d.n_lights <= 0 || !d.lights) throw PcrError(PCR_ERR_INVALID, "scene has no area light");
+    if (d.n_planes < 0 || d.n_spheres < 0 || d.n_triangles < 0 || d.n_bvh_nodes < 0)
+        throw PcrError(PCR_ERR_INVALID, "negative count in scene descriptor");
+    if ((d.n_planes && !d.planes) || (d.n_spheres && !d.spheres) || (d.n_triangles && !d.triangles))
+        throw PcrError(PCR_ERR_INVALID, "null array with non-zero count");
+    int sid = -1;
+    for (size_t i = 0; i < scenes_.size(); i++)
+        if (!scenes_[i].live) { sid = (int)i; break; }
+    if (sid < 0) {
+        if (scenes_.size() >= 256) throw PcrError(PCR_ERR_NO_MEMORY, "scene cache full (256 scenes)");
+        scenes_.emplace_back();
+        sid = (int)scenes_.size() - 1;
+    }
+    SceneEntry e;
+    e.name = d.name ? d.name : "";
+    e.version = d.version ? d.version : "";
+    std::memcpy(e.cam, d.cam_pos, sizeof(e.cam));
+    e.fov = d.fov;
+
+    // triangles + BVH (built here with the reference's builder when absent)
+    std::vector<pcr_triangle> tris(d.triangles, d.triangles + d.n_triangles);
+    std::vector<int32_t> ids(d.n_triangles);
+    for (int i = 0; i < d.n_triangles; i++) ids[i] = d.triangle_ids ? d.triangle_ids[i] : i;
+    std::vector<pcr_bvh_node> bvh;
+    if (d.n_triangles > 0) {
+        if (d.n_bvh_nodes > 0 && d.bvh_nodes)
+            bvh.assign(d.bvh_nodes, d.bvh_nodes + d.n_bvh_nodes);
+        else
+            bvh = build_bvh(tris, &ids);
+    }
+    for (const auto& n : bvh)
+        if (n.count == 0 && (n.left_or_first < 0 || n.left_or_first >= (int)bvh.size() || n.right_child < 0 ||
+                             n.right_child >= (int)bvh.size()))
+            throw PcrError(PCR_ERR_INVALID, "BVH child index out of range");
+    std::vector<DNode4> nodes4 = collapse_bvh4(bvh, d.n_triangles);
+
+    // materials
+    for (int i = 0; i < d.n_materials; i++) {
+        const pcr_material& m = d.materials[i];
+        DMaterial M{};
+        M.flags = (m.emissive[0] > 0 || m.emissive[1] > 0 || m.emissive[2] > 0 ? kMatEmissive : 0) |
+                  (m.metallic ? kMatMetallic : 0) | (m.transparent ? kMatTransparent : 0) |
+                  (m.use_tab_albedo ? kMatTabA : 0) | (m.use_tab_emissive ? kMatTabE : 0);
+        M.ior = m.ior;
+        M.cauchyB = m.cauchy_b;
+        M.albedo_max = std::max(m.albedo[0], std::max(m.albedo[1], m.albedo[2]));
+        M.albedo = make_float4(m.albedo[0], m.albedo[1], m.albedo[2], 0.f);
+        M.emissive = make_float4(m.emissive[0], m.emissive[1], m.emissive[2], 0.f);
+        M.afit = make_float4(m.albedo_fit[0], m.albedo_fit[1], m.albedo_fit[2], m.albedo_fit[3]);
+        M.efit = make_float4(m.emissive_fit[0], m.emissive_fit[1], m.emissive_fit[2], m.emissive_fit[3]);
+        for (int k = 0; k < kSpecN; k++) {
+            M.tabA[k] = m.tab_albedo[k];
+            M.tabE[k] = m.tab_emissive[k];
+        }
+        e.mats.push_back(M);
+    }
+    auto check_mat = [&](int m, const char* what) {
+        if (m < 0 || m >= d.n_materials) throw PcrError(PCR_ERR_INVALID, std::string(what) + ": material index out of range");
+    };
+
+    std::vector<DPlane> planes(d.n_planes);
+    for (int i = 0; i < d.n_planes; i++) {
+        const pcr_plane& p = d.planes[i];
+        check_mat(p.mat, "plane");
+        DPlane P;
+        P.o_mat = make_float4(p.origin[0], p.origin[1], p.origin[2], __int_as_float_host(p.mat));
+        P.n_area = make_float4(p.n[0], p.n[1], p.n[2], p.area);
+        // u.dot(u) exactly as Plane::intersect computes it (code/Includes/Plane.h:46-47)
+        float uu = p.u[0] * p.u[0] + p.u[1] * p.u[1] + p.u[2] * p.u[2];
+        float vv = p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2];
+        P.u_uu = make_float4(p.u[0], p.u[1], p.u[2], uu);
+        P.v_vv = make_float4(p.v[0], p.v[1], p.v[2], vv);
+        planes[i] = P;
+    }
+    std::vector<DSphere> spheres(d.n_spheres);
+    for (int i = 0; i < d.n_spheres; i++) {
+        const pcr_sphere& s = d.spheres[i];
+        check_mat(s.mat, "sphere");
+        spheres[i].c_r = make_float4(s.center[0], s.center[1], s.center[2], s.radius);
+        spheres[i].mat = make_int4(s.mat, 0, 0, 0);
+    }
+    auto to_dtri = [&](const pcr_triangle& t, int id) {
+        DTri T;
+        float e1[3], e2[3];
+        for (int k = 0; k < 3; k++) {
+            e1[k] = t.v1[k] - t.v0[k];
+            e2[k] = t.v2[k] - t.v0[k];
+        }
+        T.v0_id = make_float4(t.v0[0], t.v0[1], t.v0[2], __int_as_float_host(id));
+        T.e1_mat = make_float4(e1[0], e1[1], e1[2], __int_as_float_host(t.mat));
+        T.e2_flags = make_float4(e2[0], e2[1], e2[2], __int_as_float_host(t.smooth ? 1 : 0));
+        return T;
+    };
+    std::vector<DTri> dtris(d.n_triangles);
+    std::vector<float4> tri_n((size_t)d.n_triangles * 3), tri_flat(d.n_triangles);
+    for (int i = 0; i < d.n_triangles; i++) {
+        check_mat(tris[i].mat, "triangle");
+        dtris[i] = to_dtri(tris[i], ids[i]);
+        tri_n[i * 3 + 0] = make_float4(tris[i].n0[0], tris[i].n0[1], tris[i].n0[2], 0.f);
+        tri_n[i * 3 + 1] = make_float4(tris[i].n1[0], tris[i].n1[1], tris[i].n1[2], 0.f);
+        tri_n[i * 3 + 2] = make_float4(tris[i].n2[0], tris[i].n2[1], tris[i].n2[2], 0.f);
+        tri_flat[i] = make_float4(tris[i].flat_n[0], tris[i].flat_n[1], tris[i].flat_n[2], 0.f);
+    }
+    // lights
+    std::vector<DLight> lights(d.n_lights);
+    int n_lt = 0;
+    for (int i = 0; i < d.n_lights; i++) {
+        const pcr_light& L = d.lights[i];
+        if (L.kind == 1) n_lt = std::max(n_lt, L.tri_offset + L.tri_count);
+    }
+    std::vector<DTri> ltris(n_lt);
+    std::vector<float4> lflat(n_lt);
+    std::vector<float> lcum(n_lt);
+    float total_area = 0.f;
+    for (int i = 0; i < d.n_lights; i++) {
+        const pcr_light& L = d.lights[i];
+        DLight D{};
+        D.kind = L.kind;
+        D.total_area = L.total_area;
+        D.tri_offset = L.tri_offset;
+        D.tri_count = L.tri_count;
+        total_area += L.total_area;  // code/Renderer.cpp:134-136
+        if (L.kind == 0) {
+            check_mat(L.plane.mat, "light");
+            D.o_mat = make_float4(L.plane.origin[0], L.plane.origin[1], L.plane.origin[2], __int_as_float_host(L.plane.mat));
+            D.u = make_float4(L.plane.u[0], L.plane.u[1], L.plane.u[2], 0.f);
+            D.v = make_float4(L.plane.v[0], L.plane.v[1], L.plane.v[2], 0.f);
+            D.n = make_float4(L.plane.n[0], L.plane.n[1], L.plane.n[2], 0.f);
+        } else {
+            if (L.kind != 1 || L.tri_count <= 0 || L.tri_offset < 0 || !d.light_triangles || !d.light_cum_area)
+                throw PcrError(PCR_ERR_INVALID, "bad triangle-set light");
+            for (int k = L.tri_offset; k < L.tri_offset + L.tri_count; k++) {
+                check_mat(d.light_triangles[k].mat, "light triangle");
+                ltris[k] = to_dtri(d.light_triangles[k], k);
+                lflat[k] = make_float4(d.light_triangles[k].flat_n[0], d.light_triangles[k].flat_n[1],
+                                       d.light_triangles[k].flat_n[2], 0.f);
+                lcum[k] = d.light_cum_area[k];
+            }
+        }
+        lights[i] = D;
+    }
+
+    // material table growth
+    if (mat_count_ + d.n_materials > mat_cap_) {
+        int cap = std::max(mat_cap_ * 2, mat_count_ + d.n_materials);
+        DMaterial* nm = nullptr;
+        CK(cudaMalloc(&nm, sizeof(DMaterial) * cap));
+        if (mat_count_) CK(cudaMemcpy(nm, d_mats_, sizeof(DMaterial) * mat_count_, cudaMemcpyDeviceToDevice));
+        auto it = std::find(qallocs_.begin(), qallocs_.end(), (void*)d_mats_);
+        if (it != qallocs_.end()) qallocs_.erase(it);
+        CK(cudaStreamSynchronize(stream_));
+        CK(cudaFree(d_mats_));
+        d_mats_ = nm;
+        qallocs_.push_back(nm);
+        mat_cap_ = cap;
+    }
+    const int mat_base = mat_count_;
+    CK(cudaMemcpy(d_mats_ + mat_base, e.mats.data(), sizeof(DMaterial) * d.n_materials, cudaMemcpyHostToDevice));
+    mat_count_ += d.n_materials;
+
+    int64_t bytes = (int64_t)sizeof(DMaterial) * d.n_materials;
+    DScene S{};
+    S.planes = dupload(planes, e.allocs, bytes);
+    S.spheres = dupload(spheres, e.allocs, bytes);
+    S.nodes = dupload(nodes4, e.allocs, bytes);
+    S.tris = dupload(dtris, e.allocs, bytes);
+    S.tri_n = dupload(tri_n, e.allocs, bytes);
+    S.tri_flatn = dupload(tri_flat, e.allocs, bytes);
+    S.lights = dupload(lights, e.allocs, bytes);
+    S.light_tris = dupload(ltris, e.allocs, bytes);
+    S.light_flatn = dupload(lflat, e.allocs, bytes);
+    S.light_cum = dupload(lcum, e.allocs, bytes);
+    S.n_planes = d.n_planes;
+    S.n_spheres = d.n_spheres;
+    S.n_nodes = (int)nodes4.size();
+    S.n_tris = d.n_triangles;
+    S.n_lights = d.n_lights;
+    S.mat_base = mat_base;
+    S.n_mats = d.n_materials;
+    S.total_light_area = total_area;
+    e.dev = S;
+    e.bytes = bytes;
+    e.live = true;
+    CK(cudaMemcpy(d_scenes_ + sid, &S, sizeof(DScene), cudaMemcpyHostToDevice));
+    scenes_[sid] = std::move(e);
+    graph_dirty_ = true;
+    return sid;
+}
+
+void Engine::release_scene(int id)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    if (id < 0 || id >= (int)scenes_.size() || !scenes_[id].live) throw PcrError(PCR_ERR_NOT_FOUND, "unknown scene");
+    {
+        std::lock_guard<std::mutex> l(mu_);
+        for (auto& kv : reqs_)
+            if (kv.second->scene == id && (kv.second->state == ReqState::Pending || kv.second->state == ReqState::Active))
+                throw PcrError(PCR_ERR_INVALID, "scene is in use by a request");
+    }
+    CK(cudaStreamSynchronize(stream_));
+    for (void* p : scenes_[id].allocs) cudaFree(p);
+    scenes_[id].allocs.clear();
+    scenes_[id].live = false;
+    // material slots of released scenes are not compacted; the table only grows
+}
+
+int64_t Engine::scene_bytes(int id) const
+{
+    if (id < 0 || id >= (int)scenes_.size() || !scenes_[id].live) throw PcrError(PCR_ERR_NOT_FOUND, "unknown scene");
+    return scenes_[id].bytes;
+}
+
+// ---------------------------------------------------------------- requests
+void Engine::validate(int scene, const pcr_render_desc& d) const
+{
+    if (scene < 0 || scene >= (int)scenes_.size() || !scenes_[scene].live) throw PcrError(PCR_ERR_NOT_FOUND, "unknown scene");
+    if (d.width <= 0 || d.height <= 0 || d.depth <= 0 || d.samples <= 0 || d.shadow_samples <= 0)
+        throw PcrError(PCR_ERR_INVALID, "width, height, depth, samples and shadow samples must be positive");
+    if (d.depth > 255) throw PcrError(PCR_ERR_INVALID, "depth above 255");
+    if (d.shadow_samples > kMaxShadow) throw PcrError(PCR_ERR_INVALID, "more than 64 shadow samples per hit");
+    const int64_t px = (int64_t)d.width * d.height;
+    const int64_t ppp = (int64_t)d.samples * std::max(1, d.aa_samples);
+    if (px >= (1ll << 31) || ppp >= (1ll << 31) || px * ppp >= (1ll << 62))
+        throw PcrError(PCR_ERR_INVALID, "render too large");
+    if (d.shadow_samples > 8 && (int64_t)tune_.queue_capacity * 4 * d.shadow_samples > (int64_t)shadow_cap_)
+        throw PcrError(PCR_ERR_INVALID, "shadow samples exceed the shadow queue sizing");
+}
+
+int64_t Engine::request_bytes(const pcr_render_desc& d) const
+{
+    const int64_t px = (int64_t)d.width * d.height;
+    return px * 3 * (8 + 4 + 1);
+}
+
+int64_t Engine::submit(int scene, const pcr_render_desc& desc)
+{
+    validate(scene, desc);
+    auto r = std::make_unique<Request>();
+    r->scene = scene;
+    r->desc = desc;
+    r->bytes = request_bytes(desc);
+    if (r->bytes > budget_) throw PcrError(PCR_ERR_NO_MEMORY, "request larger than the device memory budget");
+    r->t_submit = std::chrono::steady_clock::now();
+    int64_t id;
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        id = next_id_++;
+        r->id = id;
+        reqs_[id] = std::move(r);
+        pending_.push_back(id);
+    }
+    cv_.notify_all();
+    return id;
+}
+
+void Engine::activate(Request& r, int slot)
+{
+    const pcr_render_desc& d = r.desc;
+    const int64_t px = (int64_t)d.width * d.height;
+    CK(cudaMallocAsync(&r.accum, px * 3 * sizeof(double), stream_));
+    CK(cudaMemsetAsync(r.accum, 0, px * 3 * sizeof(double), stream_));
+    CK(cudaMallocAsync(&r.d_hdr, px * 3 * sizeof(float), stream_));
+    CK(cudaMallocAsync(&r.d_rgb, px * 3, stream_));
+    const SceneEntry& S = scenes_[r.scene];
+    DRequest R{};
+    R.scene = r.scene;
+    R.width = d.width;
+    R.height = d.height;
+    R.depth = d.depth;
+    R.aa = std::max(1, d.aa_samples);
+    R.spp = d.samples;
+    R.paths_per_pixel = R.aa * R.spp;
+    R.shadow = d.shadow_samples;
+    R.flags = (d.spectral ? kReqSpectral : 0) | (d.mis ? kReqMIS : 0) | (d.russian ? kReqRussian : 0) |
+              (d.stratified ? kReqStratified : 0);
+    R.hero = std::min(4, std::max(1, d.hero_samples <= 0 ? 4 : d.hero_samples));
+    R.strata = d.stratified ? std::max(1, (int)std::lround(std::sqrt((float)d.samples))) : 0;
+    R.cam_x = S.cam[0];
+    R.cam_y = S.cam[1];
+    R.cam_z = S.cam[2];
+    // code/Renderer.cpp:149-150
+    R.aspect = d.width / (float)d.height;
+    R.scale = std::tan((float)3.14159265358979323846 / 180.f * 0.5f * S.fov);
+    const uint64_t seed = d.seed ? d.seed : 1ull;
+    R.seed_lo = (uint32_t)(seed & 0xffffffffu) * 0x9E3779B1u + 0x7F4A7C15u;
+    R.seed_hi = (uint32_t)(seed >> 32) ^ (uint32_t)(seed * 0xD1B54A32D192ED03ull >> 17);
+    R.total = px * R.paths_per_pixel;
+    R.accum = r.accum;
+    k_admit<<<1, 1, 0, stream_>>>(view(), R, slot);
+    CK(cudaGetLastError());
+    r.slot = slot;
+    r.state = ReqState::Active;
+    r.t_admit = std::chrono::steady_clock::now();
+    slot_owner_[slot] = r.id;
+    active_slots_.push_back(slot);
+    bytes_in_use_ += r.bytes;
+    active_dirty_ = true;
+}
+
+void Engine::admit_locked()
+{
+    // first fit under the slot limit and the memory budget, in submit order
+    for (auto it = pending_.begin(); it != pending_.end();) {
+        Request& r = *reqs_[*it];
+        if (r.state == ReqState::Cancelled) { it = pending_.erase(it); continue; }
+        if ((int)active_slots_.size() >= kMaxActive) break;
+        if (bytes_in_use_ + r.bytes > budget_) { ++it; continue; }
+        int slot = -1;
+        for (int s = 0; s < kMaxActive; s++)
+            if (slot_owner_[s] < 0) { slot = s; break; }
+        if (slot < 0) break;
+        activate(r, slot);
+        it = pending_.erase(it);
+    }
+}
+
+void Engine::upload_active()
+{
+    if (!active_dirty_) return;
+    ActiveList L;
+    L.n = (int)active_slots_.size();
+    for (int i = 0; i < L.n; i++) L.slots[i] = active_slots_[i];
+    k_set_active<<<1, 256, 0, stream_>>>(view(), L);
+    CK(cudaGetLastError());
+    active_dirty_ = false;
+}
+
+void Engine::grid_for(const void* kernel, int block, size_t smem, int* grid)
+{
+    int per_sm = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, block, smem));
+    *grid = std::max(1, per_sm) * sms_;
+}
+
+void Engine::launch_iteration(int cur, bool prof)
+{
+    const EngineView E = view();
+    const int B = tune_.block_size;
+    ShadeConst K{xyz_scale_};
+    if (prof) CK(cudaEventRecord(prof_ev_[0], stream_));
+    k_schedule<<<1, kSchedThreads, 0, stream_>>>(E, (const EngineParams*)d_params_, cur);
+    if (prof) CK(cudaEventRecord(prof_ev_[1], stream_));
+    k_regen<<<grid_regen_, B, 0, stream_>>>(E, cur);
+    if (prof) CK(cudaEventRecord(prof_ev_[2], stream_));
+    k_extend<<<grid_extend_, B, 0, stream_>>>(E, cur);
+    if (prof) CK(cudaEventRecord(prof_ev_[3], stream_));
+    k_shade<<<grid_shade_, B, shade_smem_, stream_>>>(E, cur, K, smem_mats_);
+    if (prof) CK(cudaEventRecord(prof_ev_[4], stream_));
+    k_shadow<<<grid_shadow_, B, 0, stream_>>>(E);
+    if (prof) CK(cudaEventRecord(prof_ev_[5], stream_));
+    k_status<<<1, 1024, 0, stream_>>>(E, cur ^ 1);
+    if (prof) CK(cudaEventRecord(prof_ev_[6], stream_));
+    CK(cudaGetLastError());
+    if (prof) {
+        CK(cudaEventSynchronize(prof_ev_[6]));
+        // stage index: 0 regen 1 extend 2 shade 3 shadow 4 resolve 5 schedule 6 status
+        const int map[6] = {5, 0, 1, 2, 3, 6};
+        for (int k = 0; k < 6; k++) {
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, prof_ev_[k], prof_ev_[k + 1]));
+            stage_ms_[map[k]] += ms;
+            stage_launches_[map[k]]++;
+        }
+    } else {
+        for (int k : {0, 1, 2, 3, 5, 6}) stage_launches_[k]++;
+    }
+    iterations_++;
+}
+
+void Engine::build_graph()
+{
+    const int B = tune_.block_size;
+    // materials staged in shared memory when they fit
+    const size_t mat_bytes = sizeof(DMaterial) * (size_t)std::max(1, mat_count_);
+    smem_mats_ = mat_bytes <= 96 * 1024 ? 1 : 0;
+    shade_smem_ = smem_mats_ ? mat_bytes : 0;
+    CK(cudaFuncSetAttribute(k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(shade_smem_, 0)));
+    grid_for((const void*)k_regen, B, 0, &grid_regen_);
+    grid_for((const void*)k_extend, B, 0, &grid_extend_);
+    grid_for((const void*)k_shade, B, shade_smem_, &grid_shade_);
+    grid_for((const void*)k_shadow, B, 0, &grid_shadow_);
+    if (graph_exec_) {
+        cudaGraphExecDestroy(graph_exec_);
+        graph_exec_ = nullptr;
+    }
+    if (use_graph_) {
+        cudaGraph_t g;
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        for (int it = 0; it < tune_.iters_per_launch; it++) launch_iteration(it & 1, false);
+        CK(cudaStreamEndCapture(stream_, &g));
+        CK(cudaGraphInstantiate(&graph_exec_, g, 0));
+        CK(cudaGraphDestroy(g));
+        // capture counted launches that did not run
+        for (int k : {0, 1, 2, 3, 5, 6}) stage_launches_[k] -= tune_.iters_per_launch;
+        iterations_ -= tune_.iters_per_launch;
+    }
+    graph_dirty_ = false;
+}
+
+void Engine::launch_block()
+{
+    if (graph_dirty_) build_graph();
+    if (use_graph_ && !profile_) {
+        CK(cudaGraphLaunch(graph_exec_, stream_));
+        for (int k : {0, 1, 2, 3, 5, 6}) stage_launches_[k] += tune_.iters_per_launch;
+        iterations_ += tune_.iters_per_launch;
+    } else {
+        for (int it = 0; it < tune_.iters_per_launch; it++) launch_iteration(it & 1, profile_);
+    }
+}
+
+void Engine::check_status()
+{
+    if (h_snap_->cnt.status)
+        throw PcrError(PCR_ERR_DEVICE_STATUS, "device reported queue overflow (status " +
+                                                  std::to_string(h_snap_->cnt.status) + ")");
+}
+
+void Engine::finish_request(Request& r)
+{
+    const pcr_render_desc& d = r.desc;
+    const int64_t px = (int64_t)d.width * d.height;
+    const double inv = 1.0 / ((double)d.samples * std::max(1, d.aa_samples));
+    int grid = std::min<int64_t>((px + 255) / 256, (int64_t)sms_ * 8);
+    k_resolve<<<std::max(1, grid), 256, 0, stream_>>>(r.accum, (int)px, inv, d.spectral ? 1 : 0, d.aces ? 1 : 0,
+                                                       r.d_hdr, r.d_rgb);
+    CK(cudaGetLastError());
+    if (!r.h_hdr) CK(cudaMallocHost(&r.h_hdr, px * 3 * sizeof(float)));
+    if (!r.h_rgb) CK(cudaMallocHost(&r.h_rgb, px * 3));
+    CK(cudaMemcpyAsync(r.h_hdr, r.d_hdr, px * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(r.h_rgb, r.d_rgb, px * 3, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaFreeAsync(r.accum, stream_));
+    CK(cudaFreeAsync(r.d_hdr, stream_));
+    CK(cudaFreeAsync(r.d_rgb, stream_));
+    r.accum = nullptr;
+    r.d_hdr = nullptr;
+    r.d_rgb = nullptr;
+    if (!r.ev_ready) CK(cudaEventCreateWithFlags(&r.ev_ready, cudaEventDisableTiming));
+    CK(cudaEventRecord(r.ev_ready, stream_));
+    r.state = ReqState::Resolving;
+}
+
+void Engine::harvest(bool)
+{
+    // h_snap_ holds the device state at the end of the last block
+    check_status();
+    std::vector<int> keep;
+    for (int s : active_slots_) {
+        Request& r = *reqs_[slot_owner_[s]];
+        if (h_snap_->done[s]) {
+            const unsigned long long tf = h_snap_->tf[s], td = h_snap_->td[s];
+            r.device_ms = (td > tf && tf) ? (double)(td - tf) * 1e-6 : 0.0;
+            r.paths = (uint64_t)r.desc.width * r.desc.height * r.desc.samples * std::max(1, r.desc.aa_samples);
+            finish_request(r);
+            slot_owner_[s] = -1;
+            bytes_in_use_ -= r.bytes;
+            active_dirty_ = true;
+        } else {
+            keep.push_back(s);
+        }
+    }
+    active_slots_.swap(keep);
+    // results whose copies completed
+    bool any = false;
+    for (auto& kv : reqs_) {
+        Request& r = *kv.second;
+        if (r.state == ReqState::Resolving && cudaEventQuery(r.ev_ready) == cudaSuccess) {
+            r.state = ReqState::Ready;
+            r.t_ready = std::chrono::steady_clock::now();
+            any = true;
+        }
+    }
+    if (any) cv_done_.notify_all();
+}
+
+// One round of the device loop.  Returns false when nothing is left to do.
+bool Engine::engine_step()
+{
+    CK(cudaSetDevice(device_));
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        admit_locked();
+        upload_active();
+        bool resolving = false;
+        for (auto& kv : reqs_)
+            if (kv.second->state == ReqState::Resolving) { resolving = true; break; }
+        if (active_slots_.empty()) {
+            if (resolving) {
+                CK(cudaStreamSynchronize(stream_));
+                harvest(true);
+            }
+            return !pending_.empty();
+        }
+    }
+    launch_block();
+    CK(cudaMemcpyAsync(&h_snap_->cnt, d_cnt_, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_snap_->done, d_done_, sizeof(int) * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_snap_->tf, d_tfirst_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(h_snap_->td, d_tdone_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaEventRecord(ev_snap_, stream_));
+    CK(cudaEventSynchronize(ev_snap_));
+    std::lock_guard<std::mutex> g(mu_);
+    harvest(false);
+    return true;
+}
+
+void Engine::run_until_idle()
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    if (serving_) throw PcrError(PCR_ERR_INVALID, "engine is serving on its own thread");
+    int64_t guard = 0;
+    uint64_t last_paths = ~0ull;
+    while (engine_step()) {
+        // no-progress guard: the loop must make progress every few blocks
+        if (h_snap_->cnt.paths == last_paths && h_snap_->cnt.queue_n[0] == 0 && h_snap_->cnt.queue_n[1] == 0) {
+            if (++guard > 64) throw PcrError(PCR_ERR_TIMEOUT, "engine made no progress");
+        } else {
+            guard = 0;
+        }
+        last_paths = h_snap_->cnt.paths;
+    }
+    CK(cudaStreamSynchronize(stream_));
+    std::lock_guard<std::mutex> l(mu_);
+    harvest(true);
+}
+
+void Engine::serve_loop()
+{
+    try {
+        cudaSetDevice(device_);
+        while (!stop_) {
+            bool work;
+            {
+                std::lock_guard<std::mutex> g(run_mu_);
+                work = engine_step();
+            }
+            if (!work) {
+                std::unique_lock<std::mutex> l(mu_);
+                cv_.wait_for(l, std::chrono::milliseconds(2), [&] { return stop_.load() || !pending_.empty(); });
+            }
+        }
+    } catch (const std::exception& e) {
+        std::fprintf(stderr, "pcr: serve loop stopped: %s\n", e.what());
+        serving_ = false;
+    }
+}
+
+void Engine::serve_start()
+{
+    if (serving_) return;
+    stop_ = false;
+    serving_ = true;
+    serve_thread_ = std::thread([this] { serve_loop(); });
+}
+
+void Engine::serve_stop()
+{
+    if (!serve_thread_.joinable()) return;
+    stop_ = true;
+    cv_.notify_all();
+    serve_thread_.join();
+    serving_ = false;
+}
+
+bool Engine::poll(int64_t id)
+{
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) throw PcrError(PCR_ERR_NOT_FOUND, "unknown request");
+    Request& r = *it->second;
+    if (r.state == ReqState::Resolving && cudaEventQuery(r.ev_ready) == cudaSuccess) {
+        r.state = ReqState::Ready;
+        r.t_ready = std::chrono::steady_clock::now();
+    }
+    return r.state == ReqState::Ready;
+}
+
+void Engine::wait(int64_t id, int64_t timeout_ms)
+{
+    auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms < 0 ? (int64_t)1 << 40 : timeout_ms);
+    while (!poll(id)) {
+        if (std::chrono::steady_clock::now() > deadline) throw PcrError(PCR_ERR_TIMEOUT, "wait timed out");
+        if (!serving_) {
+            std::lock_guard<std::mutex> g(run_mu_);
+            if (!engine_step()) {
+                CK(cudaStreamSynchronize(stream_));
+                std::lock_guard<std::mutex> l(mu_);
+                harvest(true);
+            }
+        } else {
+            std::unique_lock<std::mutex> l(mu_);
+            cv_done_.wait_for(l, std::chrono::milliseconds(1));
+        }
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            if (reqs_[id]->state == ReqState::Cancelled) throw PcrError(PCR_ERR_CANCELLED, "request cancelled");
+        }
+    }
+}
+
+void Engine::fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st)
+{
+    if (!poll(id)) throw PcrError(PCR_ERR_INVALID, "request not finished");
+    std::lock_guard<std::mutex> g(mu_);
+    Request& r = *reqs_[id];
+    const int64_t px = (int64_t)r.desc.width * r.desc.height;
+    if (hdr) std::memcpy(hdr, r.h_hdr, px * 3 * sizeof(float));
+    if (rgb) std::memcpy(rgb, r.h_rgb, px * 3);
+    if (st) {
+        st->device_ms = r.device_ms;
+        st->latency_ms = std::chrono::duration<double, std::milli>(r.t_ready - r.t_submit).count();
+        st->queue_ms = std::chrono::duration<double, std::milli>(r.t_admit - r.t_submit).count();
+        st->paths = r.paths;
+        st->rays = 0;
+        st->shadow_rays = 0;
+    }
+    if (r.h_hdr) cudaFreeHost(r.h_hdr);
+    if (r.h_rgb) cudaFreeHost(r.h_rgb);
+    if (r.ev_ready) cudaEventDestroy(r.ev_ready);
+    reqs_.erase(id);
+}
+
+void Engine::cancel(int64_t id)
+{
+    std::lock_guard<std::mutex> g(mu_);
+    auto it = reqs_.find(id);
+    if (it == reqs_.end()) throw PcrError(PCR_ERR_NOT_FOUND, "unknown request");
+    if (it->second->state == ReqState::Pending) {
+        it->second->state = ReqState::Cancelled;
+        return;
+    }
+    throw PcrError(PCR_ERR_INVALID, "only pending requests can be cancelled");
+}
+
+// ---------------------------------------------------------------- plain method
+void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, uint8_t* rgb, pcr_render_stats* st)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    validate(scene, desc);
+    if (!active_slots_.empty() || serving_) throw PcrError(PCR_ERR_INVALID, "plain render while batched work is active");
+    auto t0 = std::chrono::steady_clock::now();
+    Request r;
+    r.id = -1;
+    r.scene = scene;
+    r.desc = desc;
+    r.bytes = request_bytes(desc);
+    if (r.bytes > budget_) throw PcrError(PCR_ERR_NO_MEMORY, "request larger than the device memory budget");
+    if (graph_dirty_) build_graph();
+    EngineParams p{tune_.queue_capacity, tune_.queue_capacity, 1, 1};
+    k_set_params<<<1, 1, 0, stream_>>>((EngineParams*)d_params_, p);
+    activate(r, 0);
+    slot_owner_[0] = -1;  // the plain request is not in the request map
+    upload_active();
+    const int64_t total = (int64_t)desc.width * desc.height * desc.samples * std::max(1, desc.aa_samples);
+    const int64_t passes = (total + tune_.queue_capacity - 1) / tune_.queue_capacity;
+    int cur = 0;
+    for (int64_t it = 0; it < passes * (int64_t)desc.depth; it++) {
+        launch_iteration(cur, profile_);
+        cur ^= 1;
+    }
+    int extra = 0;
+    while (true) {
+        int done = 0;
+        CK(cudaMemcpyAsync(&done, d_done_, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        Counters c;
+        CK(cudaMemcpy(&c, d_cnt_, sizeof(c), cudaMemcpyDeviceToHost));
+        if (c.status) throw PcrError(PCR_ERR_DEVICE_STATUS, "device reported queue overflow");
+        if (done) break;
+        if (++extra > 4 * desc.depth + 8) throw PcrError(PCR_ERR_TIMEOUT, "plain render did not finish");
+        launch_iteration(cur, profile_);
+        cur ^= 1;
+    }
+    // a plain render always ends on queue parity 0 for the next user
+    if (cur != 0) {
+        launch_iteration(cur, false);
+        cur ^= 1;
+    }
+    unsigned long long tf = 0, td = 0;
+    CK(cudaMemcpy(&tf, d_tfirst_, 8, cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(&td, d_tdone_, 8, cudaMemcpyDeviceToHost));
+    finish_request(r);
+    CK(cudaStreamSynchronize(stream_));
+    active_slots_.clear();
+    active_dirty_ = true;
+    bytes_in_use_ -= r.bytes;
+    upload_active();
+    EngineParams q{tune_.queue_capacity, tune_.chunk_paths, tune_.regen_every, 0};
+    k_set_params<<<1, 1, 0, stream_>>>((EngineParams*)d_params_, q);
+    CK(cudaStreamSynchronize(stream_));
+    const int64_t px = (int64_t)desc.width * desc.height;
+    if (hdr) std::memcpy(hdr, r.h_hdr, px * 3 * sizeof(float));
+    if (rgb) std::memcpy(rgb, r.h_rgb, px * 3);
+    cudaFreeHost(r.h_hdr);
+    cudaFreeHost(r.h_rgb);
+    cudaEventDestroy(r.ev_ready);
+    if (st) {
+        st->device_ms = (td > tf && tf) ? (double)(td - tf) * 1e-6 : 0.0;
+        st->latency_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        st->queue_ms = 0;
+        st->paths = (uint64_t)total;
+        st->rays = 0;
+        st->shadow_rays = 0;
+    }
+}
+
+// ---------------------------------------------------------------- parity entry points
+void Engine::trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_t* prim, float* t, int bvh_only,
+                   int32_t* counts)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    if (scene < 0 || scene >= (int)scenes_.size() || !scenes_[scene].live) throw PcrError(PCR_ERR_NOT_FOUND, "unknown scene");
+    if (n <= 0) return;
+    float* d_rays = nullptr;
+    int *d_mat = nullptr, *d_prim = nullptr, *d_cnt = nullptr;
+    float* d_t = nullptr;
+    CK(cudaMallocAsync(&d_rays, n * 6 * sizeof(float), stream_));
+    CK(cudaMallocAsync(&d_mat, n * sizeof(int), stream_));
+    CK(cudaMallocAsync(&d_prim, n * sizeof(int), stream_));
+    CK(cudaMallocAsync(&d_t, n * sizeof(float), stream_));
+    if (counts) CK(cudaMallocAsync(&d_cnt, n * 2 * sizeof(int), stream_));
+    CK(cudaMemcpyAsync(d_rays, rays, n * 6 * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    int grid = 0;
+    grid_for((const void*)k_trace_rays, 128, 0, &grid);
+    k_trace_rays<<<grid, 128, 0, stream_>>>(d_scenes_ + scene, d_mats_, d_rays, n, d_mat, d_prim, d_t, bvh_only, d_cnt);
+    CK(cudaGetLastError());
+    if (mat) CK(cudaMemcpyAsync(mat, d_mat, n * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    if (prim) CK(cudaMemcpyAsync(prim, d_prim, n * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    if (t) CK(cudaMemcpyAsync(t, d_t, n * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    if (counts) CK(cudaMemcpyAsync(counts, d_cnt, n * 2 * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaFreeAsync(d_rays, stream_));
+    CK(cudaFreeAsync(d_mat, stream_));
+    CK(cudaFreeAsync(d_prim, stream_));
+    CK(cudaFreeAsync(d_t, stream_));
+    if (d_cnt) CK(cudaFreeAsync(d_cnt, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::eval_stage(int what, const float* params, const float* in, int64_t n, float* out)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    if (what < 0 || what > 7 || n <= 0) throw PcrError(PCR_ERR_INVALID, "bad stage evaluation request");
+    const int in_w = (what == 0 || what == 1 || what == 2) ? 1 : (what == 3 ? 2 : 3);
+    const int out_w = (what == 0 || what == 1) ? 1 : 3;
+    const int np = what == 0 ? 4 : (what == 1 ? kSpecN : 0);
+    float *d_in = nullptr, *d_out = nullptr, *d_p = nullptr;
+    CK(cudaMallocAsync(&d_in, n * in_w * sizeof(float), stream_));
+    CK(cudaMallocAsync(&d_out, n * out_w * sizeof(float), stream_));
+    CK(cudaMallocAsync(&d_p, 64 * sizeof(float), stream_));
+    CK(cudaMemcpyAsync(d_in, in, n * in_w * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    if (np) {
+        if (!params) throw PcrError(PCR_ERR_INVALID, "stage needs parameters");
+        CK(cudaMemcpyAsync(d_p, params, np * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    }
+    k_eval_stage<<<std::min<int64_t>((n + 255) / 256, 4096), 256, 0, stream_>>>(what, d_p, d_in, n, d_out, xyz_scale_);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(out, d_out, n * out_w * sizeof(float), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaFreeAsync(d_in, stream_));
+    CK(cudaFreeAsync(d_out, stream_));
+    CK(cudaFreeAsync(d_p, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+// ---------------------------------------------------------------- stats / tuning
+void Engine::stats(pcr_engine_stats* o)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    Counters c;
+    CK(cudaMemcpy(&c, d_cnt_, sizeof(c), cudaMemcpyDeviceToHost));
+    std::memset(o, 0, sizeof(*o));
+    for (int k = 0; k < 8; k++) {
+        o->stage_ms[k] = stage_ms_[k];
+        o->stage_launches[k] = stage_launches_[k];
+    }
+    o->iterations = iterations_;
+    o->paths = (int64_t)(c.paths - base_paths_);
+    o->rays = (int64_t)(c.rays - base_rays_);
+    o->shadow_rays = (int64_t)(c.shadow_rays - base_shadow_);
+    size_t fr = 0, tot = 0;
+    cudaMemGetInfo(&fr, &tot);
+    o->device_bytes = (int64_t)(tot - fr);
+    o->queue_capacity = tune_.queue_capacity;
+    o->block_size = tune_.block_size;
+    o->chunk_paths = tune_.chunk_paths;
+    o->regen_every = tune_.regen_every;
+}
+
+void Engine::reset_stats()
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    Counters c;
+    CK(cudaMemcpy(&c, d_cnt_, sizeof(c), cudaMemcpyDeviceToHost));
+    base_paths_ = c.paths;
+    base_rays_ = c.rays;
+    base_shadow_ = c.shadow_rays;
+    std::memset(stage_ms_, 0, sizeof(stage_ms_));
+    std::memset(stage_launches_, 0, sizeof(stage_launches_));
+    iterations_ = 0;
+}
+
+// ---------------------------------------------------------------- autotuner
+// Times short trial batches of the caller's sample workload under a small
+// grid of (queue capacity, block size, issue chunk, refill cadence) and keeps
+// the fastest.  The choice is written to the tuning cache file when one was
+// given at context creation.
+void Engine::autotune(const int32_t* scenes, const pcr_render_desc* descs, int n, int32_t* chosen)
+{
+    struct Cand { int q, b, c, r; };
+    std::vector<Cand> cands;
+    for (int q : {1 << 19, 1 << 20, 1 << 21})
+        for (int b : {64, 128, 256})
+            for (int c : {1 << 14, 1 << 16})
+                for (int r : {1, 2}) cands.push_back({q, b, c, r});
+    EngineTuning best = tune_;
+    double best_ms = 1e30;
+    cudaEvent_t a, z;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&z));
+    for (const Cand& cd : cands) {
+        EngineTuning t = tune_;
+        t.queue_capacity = cd.q;
+        t.block_size = cd.b;
+        t.chunk_paths = cd.c;
+        t.regen_every = cd.r;
+        set_tuning(t);
+        std::vector<int64_t> ids;
+        for (int i = 0; i < n; i++) ids.push_back(submit(scenes[i], descs[i]));
+        CK(cudaEventRecord(a, stream_));
+        run_until_idle();
+        CK(cudaEventRecord(z, stream_));
+        CK(cudaEventSynchronize(z));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, a, z));
+        for (int64_t id : ids) fetch(id, nullptr, nullptr, nullptr);
+        if (ms < best_ms) { best_ms = ms; best = t; }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    set_tuning(best);
+    if (chosen) {
+        chosen[0] = best.queue_capacity;
+        chosen[1] = best.block_size;
+        chosen[2] = best.chunk_paths;
+        chosen[3] = best.regen_every;
+    }
+    if (!tuning_cache_.empty()) {
+        if (FILE* f = std::fopen(tuning_cache_.c_str(), "w")) {
+            std::fprintf(f, "{\"queue_capacity\": %d, \"block_size\": %d, \"chunk_paths\": %d, \"regen_every\": %d, \"ms\": %.3f}\n",
+                         best.queue_capacity, best.block_size, best.chunk_paths, best.regen_every, best_ms);
+            std::fclose(f);
+        }
+    }
+}
+
+}  // namespace pcr

@@ -1,0 +1,183 @@
+// Host side of the wavefront engine: device scene cache, request table,
+// admission under a memory budget, the graph-captured iteration loop
+// (batched / served method) and the plain per-request launch sequence.
+#pragma once
+
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstdint>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/pcr_cuda.h"
+#include "layout.h"
+
+namespace pcr {
+
+struct PcrError : std::runtime_error {
+    pcr_status status;
+    PcrError(pcr_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+struct SceneEntry {
+    DScene dev{};
+    std::vector<void*> allocs;
+    int64_t bytes = 0;
+    std::string name, version;
+    float cam[3] = {0, 0, 0}, fov = 65.f;
+    std::vector<DMaterial> mats;
+    bool live = false;
+};
+
+enum class ReqState { Pending, Active, Resolving, Ready, Fetched, Cancelled };
+
+struct Request {
+    int64_t id = 0;
+    int scene = 0;
+    pcr_render_desc desc{};
+    ReqState state = ReqState::Pending;
+    int slot = -1;
+    int64_t bytes = 0;
+    double* accum = nullptr;
+    float* d_hdr = nullptr;
+    uint8_t* d_rgb = nullptr;
+    float* h_hdr = nullptr;      // pinned
+    uint8_t* h_rgb = nullptr;    // pinned
+    cudaEvent_t ev_ready = nullptr;
+    std::chrono::steady_clock::time_point t_submit, t_admit, t_ready;
+    double device_ms = 0;
+    uint64_t paths = 0;
+};
+
+struct EngineTuning {
+    int queue_capacity = 1 << 20;  // fill target
+    int block_size = 128;
+    int chunk_paths = 1 << 16;
+    int regen_every = 1;
+    int iters_per_launch = 8;      // iterations per graph launch (even)
+};
+
+class Engine {
+public:
+    explicit Engine(const pcr_ctx_opts* opts);
+    ~Engine();
+
+    int upload_scene(const pcr_scene_desc& d);
+    void release_scene(int id);
+    int64_t scene_bytes(int id) const;
+
+    void render_plain(int scene, const pcr_render_desc& desc, float* hdr, uint8_t* rgb, pcr_render_stats* st);
+    int64_t submit(int scene, const pcr_render_desc& desc);
+    void run_until_idle();
+    void serve_start();
+    void serve_stop();
+    bool poll(int64_t id);
+    void wait(int64_t id, int64_t timeout_ms);
+    void fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st);
+    void cancel(int64_t id);
+
+    void trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_t* prim, float* t, int bvh_only,
+               int32_t* counts);
+    void eval_stage(int what, const float* params, const float* in, int64_t n, float* out);
+
+    void stats(pcr_engine_stats* out);
+    void reset_stats();
+    void set_tuning(const EngineTuning& t);
+    const EngineTuning& tuning() const { return tune_; }
+    void autotune(const int32_t* scenes, const pcr_render_desc* descs, int n, int32_t* chosen);
+    int device() const { return device_; }
+    cudaStream_t stream() const { return stream_; }
+
+private:
+    void alloc_buffers();
+    void free_buffers();
+    void validate(int scene, const pcr_render_desc& d) const;
+    int64_t request_bytes(const pcr_render_desc& d) const;
+    void admit_locked();
+    void activate(Request& r, int slot);
+    void upload_active();
+    void launch_iteration(int cur, bool profile);
+    void launch_block();
+    void build_graph();
+    void harvest(bool final_sync);
+    void finish_request(Request& r);
+    void check_status();
+    bool engine_step();
+    void serve_loop();
+    EngineView view() const;
+    void grid_for(const void* kernel, int block, size_t smem, int* grid);
+
+    int device_ = 0;
+    int sms_ = 148;
+    cudaStream_t stream_ = nullptr;
+    EngineTuning tune_;
+    bool use_graph_ = true, profile_ = false;
+    int64_t budget_ = 40ll << 30;
+    std::string tuning_cache_;
+
+    // scenes
+    std::vector<SceneEntry> scenes_;
+    DScene* d_scenes_ = nullptr;
+    DMaterial* d_mats_ = nullptr;
+    int mat_cap_ = 0, mat_count_ = 0;
+    float xyz_scale_ = 0.f;
+
+    // request table
+    DRequest* d_reqs_ = nullptr;
+    DRequest* h_reqs_ = nullptr;  // pinned mirror
+    unsigned long long *d_issued_ = nullptr, *d_tfirst_ = nullptr, *d_tdone_ = nullptr;
+    long long* d_outstanding_ = nullptr;
+    long long* d_give_start_ = nullptr;
+    int *d_give_ = nullptr, *d_give_base_ = nullptr, *d_active_ = nullptr, *d_nactive_ = nullptr, *d_done_ = nullptr;
+    int* h_active_ = nullptr;     // pinned: [0] = n, then slots
+    Counters* d_cnt_ = nullptr;
+    struct HostSnap { Counters cnt; int done[kMaxActive]; unsigned long long tf[kMaxActive], td[kMaxActive]; };
+    HostSnap* h_snap_ = nullptr;  // pinned
+    cudaEvent_t ev_snap_ = nullptr;
+    void* d_params_ = nullptr;
+    void* h_params_ = nullptr;
+
+    // queues
+    PathQueue q_[2]{};
+    float4* d_hit_ = nullptr;
+    ShadowQueue sq_{};
+    int queue_cap_ = 0, shadow_cap_ = 0;
+    std::vector<void*> qallocs_;
+
+    // graph
+    cudaGraphExec_t graph_exec_ = nullptr;
+    bool graph_dirty_ = true;
+    int grid_regen_ = 0, grid_extend_ = 0, grid_shade_ = 0, grid_shadow_ = 0;
+    size_t shade_smem_ = 0;
+    int smem_mats_ = 0;
+
+    // requests
+    std::mutex mu_;
+    std::condition_variable cv_, cv_done_;
+    std::map<int64_t, std::unique_ptr<Request>> reqs_;
+    std::deque<int64_t> pending_;
+    std::vector<int64_t> slot_owner_;   // request id per slot (-1 free)
+    std::vector<int> active_slots_;
+    int64_t next_id_ = 1;
+    int64_t bytes_in_use_ = 0;
+    bool active_dirty_ = true;
+    std::thread serve_thread_;
+    std::atomic<bool> serving_{false}, stop_{false};
+    std::mutex run_mu_;   // one driver of the device loop at a time
+
+    // stats
+    double stage_ms_[8] = {0};
+    int64_t stage_launches_[8] = {0};
+    int64_t iterations_ = 0;
+    uint64_t base_rays_ = 0, base_shadow_ = 0, base_paths_ = 0;
+    cudaEvent_t prof_ev_[16]{};
+};
+
+}  // namespace pcr

@@ -1,0 +1,721 @@
+// Wavefront stage kernels.  One iteration of the persistent wavefront is
+//   schedule -> regen -> extend -> shade -> shadow -> status
+// over the current path queue; shade writes surviving paths into the other
+// queue.  Every kernel is a grid-stride loop over a device-side count, so
+// a whole iteration (and several in a row) can be captured in one CUDA
+// graph with no host round trip.  No kernel waits on another block or on
+// the host: there is no spin anywhere.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cooperative_groups/scan.h>
+#include <cub/block/block_scan.cuh>
+
+#include "device.cuh"
+
+namespace pcr {
+
+struct EngineParams {
+    int fill;          // refill target (paths in flight)
+    int chunk;         // per-request issue chunk per refill
+    int regen_every;   // refill cadence in iterations
+    int plain;         // 1: refill only when the queue is empty (pass-wise)
+};
+
+// ------------------------------------------------------------------ schedule
+// One block.  Decides how many new camera paths each active request gets
+// this iteration: first up to `chunk` each (round-robin fairness), then the
+// remaining free slots oldest-first.
+constexpr int kSchedThreads = 1024;
+
+__global__ void __launch_bounds__(kSchedThreads) k_schedule(EngineView E, const EngineParams* P, int cur)
+{
+    typedef cub::BlockScan<long long, kSchedThreads> Scan;
+    __shared__ typename Scan::TempStorage tmp;
+    __shared__ long long s_total;
+    Counters* C = E.cnt;
+    const int tid = threadIdx.x;
+    const int n_act = *E.n_active;
+    int qn = C->queue_n[cur];
+    if (qn > E.queue_cap) {  // never expected: shade guards every append
+        qn = E.queue_cap;
+        if (tid == 0) atomicOr(&C->status, 4);
+    }
+    const EngineParams p = *P;
+    long long free_slots = (long long)p.fill - qn;
+    if (free_slots < 0) free_slots = 0;
+    if (p.plain && qn > 0) free_slots = 0;
+    if (p.regen_every > 1 && (C->iter % p.regen_every) != 0 && qn > 0) free_slots = 0;
+
+    int slot = -1;
+    long long rem = 0;
+    if (tid < n_act) {
+        slot = E.active[tid];
+        rem = E.reqs[slot].total - (long long)E.issued[slot];
+        if (rem < 0) rem = 0;
+    }
+    // pass 1: up to chunk each, in active order
+    long long w1 = rem < (long long)p.chunk ? rem : (long long)p.chunk;
+    long long ex1, tot1;
+    Scan(tmp).ExclusiveSum(w1, ex1, tot1);
+    __syncthreads();
+    long long g1 = free_slots - ex1;
+    g1 = g1 < 0 ? 0 : (g1 > w1 ? w1 : g1);
+    long long left = free_slots - (tot1 < free_slots ? tot1 : free_slots);
+    long long rem2 = rem - g1;
+    long long ex2, tot2;
+    Scan(tmp).ExclusiveSum(rem2, ex2, tot2);
+    __syncthreads();
+    long long g2 = left - ex2;
+    g2 = g2 < 0 ? 0 : (g2 > rem2 ? rem2 : g2);
+    long long g = g1 + g2;
+    long long exg, totg;
+    Scan(tmp).ExclusiveSum(g, exg, totg);
+    if (tid < n_act) {
+        E.give[tid] = (int)g;
+        E.give_base[tid] = (int)exg;
+        E.give_start[tid] = (long long)E.issued[slot];
+        if (g > 0) {
+            if (E.issued[slot] == 0ull) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                E.t_first[slot] = t;
+            }
+            E.issued[slot] += (unsigned long long)g;
+            E.outstanding[slot] += g;
+        }
+    }
+    if (tid == 0) s_total = totg;
+    __syncthreads();
+    if (tid == 0) {
+        C->new_base = qn;
+        C->new_n = (int)s_total;
+        C->queue_n[cur] = qn + (int)s_total;
+        C->queue_n[cur ^ 1] = 0;
+        C->shadow_n = 0;
+        C->paths += (unsigned long long)s_total;
+    }
+}
+
+// ------------------------------------------------------------------ regen
+// Camera rays for the new paths (code/Renderer.cpp:190-239): pixel centre,
+// jitter when aa > 1, hero wavelength and its stratified companions.
+__global__ void k_regen(EngineView E, int cur)
+{
+    __shared__ int s_base[kMaxActive];
+    __shared__ int s_give[kMaxActive];
+    __shared__ int s_slot[kMaxActive];
+    __shared__ long long s_start[kMaxActive];
+    const Counters* C = E.cnt;
+    const int n_act = *E.n_active;
+    for (int i = threadIdx.x; i < n_act; i += blockDim.x) {
+        s_base[i] = E.give_base[i];
+        s_give[i] = E.give[i];
+        s_slot[i] = E.active[i];
+        s_start[i] = E.give_start[i];
+    }
+    __syncthreads();
+    const int n_new = C->new_n, base = C->new_base;
+    const PathQueue Q = E.q[cur];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n_new; i += gridDim.x * blockDim.x) {
+        int lo = 0, hi = n_act - 1;
+        while (lo < hi) {  // last r with base[r] <= i and give[r] > 0
+            int mid = (lo + hi + 1) >> 1;
+            if (s_base[mid] <= i) lo = mid; else hi = mid - 1;
+        }
+        while (lo > 0 && (s_give[lo] == 0 || s_base[lo] > i)) lo--;
+        const int slot = s_slot[lo];
+        const DRequest& R = E.reqs[slot];
+        const long long path = s_start[lo] + (i - s_base[lo]);
+        const uint32_t pixel = (uint32_t)(path / R.paths_per_pixel);
+        const uint32_t sample = (uint32_t)(path % R.paths_per_pixel);
+        const int px = (int)(pixel % (uint32_t)R.width), py = (int)(pixel / (uint32_t)R.width);
+        float jx = 0.f, jy = 0.f;
+        if (R.aa > 1) {
+            float4 j = rand4(R, pixel, sample / (uint32_t)R.spp, 0, 254u, 0);
+            jx = j.x - 0.5f;
+            jy = j.y - 0.5f;
+        }
+        float x = ((2 * (px + 0.5f + jx) / (float)R.width) - 1) * R.scale * R.aspect;
+        float y = -((2 * (py + 0.5f + jy) / (float)R.height) - 1) * R.scale;
+        float inv = rsqrtf(x * x + y * y + 1.f);
+        float3 d = make_float3(x * inv, y * inv, -inv);
+        float lambda0 = 0.f;
+        int nch = 4;
+        if (R.flags & kReqSpectral) {
+            float4 u = rand4(R, pixel, sample, 0, 255u, 0);
+            lambda0 = 400.f + u.x * 300.f;
+            nch = R.hero;
+        }
+        const int pos = base + i;
+        Q.o[pos] = make_float4(R.cam_x, R.cam_y, R.cam_z, lambda0);
+        Q.d[pos] = make_float4(d.x, d.y, d.z, __int_as_float(nch << 12));
+        Q.tp[pos] = make_float4(1.f, 1.f, 1.f, 1.f);
+        Q.id[pos] = make_int4(slot, (int)pixel, (int)sample, 0);
+    }
+}
+
+// ------------------------------------------------------------------ extend
+// Closest hit for every queued path (trace_closest).
+__global__ void k_extend(EngineView E, int cur)
+{
+    const Counters* C = E.cnt;
+    const int n = min(C->queue_n[cur], E.queue_cap);
+    const PathQueue Q = E.q[cur];
+    unsigned long long mine = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int slot = Q.id[i].x;
+        const DScene& S = E.scenes[E.reqs[slot].scene];
+        float4 o = Q.o[i], d = Q.d[i];
+        float t = FLT_MAX, u = 0.f, v = 0.f;
+        uint32_t prim = scene_closest(S, xyz(o), xyz(d), FLT_MAX, t, u, v);
+        E.hit[i] = make_float4(t, __uint_as_float(prim), u, v);
+        mine++;
+    }
+    for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, off);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&E.cnt->rays, mine);
+}
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ int warp_append(int* counter, bool want)
+{
+    const unsigned mask = __ballot_sync(0xffffffffu, want);
+    if (mask == 0) return -1;
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(mask) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(counter, __popc(mask));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    return want ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
+}
+
+__device__ __forceinline__ void add_xyz(double* acc, float3 c)
+{
+    atomicAdd(acc + 0, (double)c.x);
+    atomicAdd(acc + 1, (double)c.y);
+    atomicAdd(acc + 2, (double)c.z);
+}
+
+// Per-channel XYZ weights of a path's wavelengths: w_k = cmf(lam_k) *
+// (700-400)/yBarIntegral / N, so the pixel contribution of per-channel
+// radiance c is sum_k c_k w_k = sum_k singleLambdaXYZ(lam_k, c_k) / N
+// (code/Renderer.cpp:254-257, code/Includes/CIE.h:140-159).  Computed once
+// per vertex; RGB mode passes the channels through.
+struct XyzWeights {
+    float3 w[4];
+};
+__device__ __forceinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale)
+{
+    XyzWeights W;
+    if (!spectral) {
+        W.w[0] = make_float3(1.f, 0.f, 0.f);
+        W.w[1] = make_float3(0.f, 1.f, 0.f);
+        W.w[2] = make_float3(0.f, 0.f, 1.f);
+        W.w[3] = make_float3(0.f, 0.f, 0.f);
+        return W;
+    }
+    for (int k = 0; k < 4; k++) {
+        if (k < nch) {
+            float3 c = cmf(lam[k]);
+            const float s = xyz_scale * wN;
+            W.w[k] = make_float3(c.x * s, c.y * s, c.z * s);
+        } else {
+            W.w[k] = make_float3(0.f, 0.f, 0.f);
+        }
+    }
+    return W;
+}
+__device__ __forceinline__ float3 apply_xyz(const XyzWeights& W, const float* c)
+{
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = 0; k < 4; k++) {
+        s.x += c[k] * W.w[k].x;
+        s.y += c[k] * W.w[k].y;
+        s.z += c[k] * W.w[k].z;
+    }
+    return s;
+}
+
+struct ShadeConst {
+    float xyz_scale;  // (700-400) / yBarIntegral
+};
+
+// ------------------------------------------------------------------ shade
+// Per-path shading of the hit found by k_extend (code/Renderer.cpp:656-889
+// with samples = 1, the GPU's paths-per-pixel estimator): emission,
+// mirror, dielectric (with the 4-way hero fork at dispersive glass),
+// diffuse direct lighting via explicit shadow rays, Russian roulette and the
+// cosine-hemisphere continuation.  Materials are staged in shared memory.
+__global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
+{
+    extern __shared__ DMaterial s_mat[];
+    const DMaterial* M = E.mats;
+    if (smem_mats) {
+        const int words = E.n_mats * (int)(sizeof(DMaterial) / 16);
+        const float4* src = reinterpret_cast<const float4*>(E.mats);
+        float4* dst = reinterpret_cast<float4*>(s_mat);
+        for (int i = threadIdx.x; i < words; i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+        M = s_mat;
+    }
+    Counters* C = E.cnt;
+    const int n = min(C->queue_n[cur], E.queue_cap);
+    const PathQueue Q = E.q[cur];
+    const PathQueue NQ = E.q[cur ^ 1];
+    const ShadowQueue SQ = E.sq;
+    const float inv_pi = 1.f / 3.14159274f;
+    // warp-uniform trip count: every lane of a warp runs the same iterations,
+    // so the warp-wide appends at the bottom see all 32 lanes
+    const int stride = gridDim.x * blockDim.x;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
+        const int i = base + threadIdx.x;
+        const bool live = i < n;
+        int4 id = make_int4(0, 0, 0, 0);
+        float4 o4 = make_float4(0, 0, 0, 0), d4 = o4, tp4 = o4, h = o4;
+        if (live) { id = Q.id[i]; o4 = Q.o[i]; d4 = Q.d[i]; tp4 = Q.tp[i]; h = E.hit[i]; }
+        const int slot = id.x;
+        const DRequest& R = E.reqs[slot];
+        const uint32_t prim = __float_as_uint(h.y);
+        const int meta = __float_as_int(d4.w);
+        const int bounce = meta & 0xFF, fork = (meta >> 8) & 7, single = (meta >> 11) & 1, nHero = (meta >> 12) & 7;
+        const bool spectral = live && (R.flags & kReqSpectral);
+        bool cont = false;            // continue into the next queue
+        int nfork = 0;                // forked sub-paths to emit
+        float3 no = make_float3(0, 0, 0), nd = no;
+        float ntp[4] = {0, 0, 0, 0};
+        float fork_o[4][3], fork_d[4][3], fork_tp[4], fork_lam[4];
+        double* acc = nullptr;
+        float3 emit_xyz = make_float3(0, 0, 0);
+        bool emit = false;
+
+        // wavelengths carried by this path
+        float lam[4];
+        int nch = 1;
+        float wN = 1.f;
+        if (spectral) {
+            if (single) {
+                lam[0] = lam[1] = lam[2] = lam[3] = o4.w;
+                nch = 1;
+                wN = 1.f / (float)nHero;
+            } else {
+                const float span = 300.f, stride_l = span / (float)nHero;
+                lam[0] = o4.w;
+                for (int k = 1; k < 4; k++) {
+                    float l = lam[0] + stride_l * k;
+                    if (l > 700.f) l -= span;
+                    lam[k] = k < nHero ? l : lam[0];
+                }
+                nch = nHero;
+                wN = 1.f / (float)nHero;
+            }
+        } else {
+            lam[0] = lam[1] = lam[2] = lam[3] = 0.f;
+            nch = 3;
+        }
+        float tp[4] = {tp4.x, tp4.y, tp4.z, tp4.w};
+
+        if (live && (prim & kPrimKindMask) != kPrimNone) {
+            const DScene& S = E.scenes[R.scene];
+            acc = R.accum + (size_t)id.y * 3;
+            const float3 o = xyz(o4), d = xyz(d4);
+            const float t = h.x;
+            const float3 hit = make_float3(o.x + d.x * t, o.y + d.y * t, o.z + d.z * t);
+            float3 N;
+            int mi;
+            const uint32_t kind = prim & kPrimKindMask, pidx = prim & kPrimIndexMask;
+            if (kind == kPrimSphere) {
+                const float4 cr = S.spheres[pidx].c_r;
+                float3 v = make_float3(hit.x - cr.x, hit.y - cr.y, hit.z - cr.z);
+                float il = rsqrtf(f3dot(v, v));
+                N = f3mul(v, il);
+                mi = S.spheres[pidx].mat.x;
+            } else if (kind == kPrimPlane) {
+                const float4 na = S.planes[pidx].n_area;
+                N = make_float3(na.x, na.y, na.z);
+                mi = __float_as_int(S.planes[pidx].o_mat.w);
+            } else {
+                const DTri& tr = S.tris[pidx];
+                mi = __float_as_int(tr.e1_mat.w);
+                if (__float_as_int(tr.e2_flags.w) & 1) {
+                    const float4 n0 = S.tri_n[pidx * 3], n1 = S.tri_n[pidx * 3 + 1], n2 = S.tri_n[pidx * 3 + 2];
+                    const float w = 1.f - h.z - h.w;
+                    float3 in = make_float3(n0.x * w + n1.x * h.z + n2.x * h.w, n0.y * w + n1.y * h.z + n2.y * h.w,
+                                            n0.z * w + n1.z * h.z + n2.z * h.w);
+                    N = f3mul(in, rsqrtf(f3dot(in, in)));
+                } else {
+                    N = xyz(S.tri_flatn[pidx]);
+                }
+            }
+            const bool entering = f3dot(d, N) < 0.f;
+            if (!entering) N = f3neg(N);
+            const DMaterial& m = M[S.mat_base + mi];
+            const bool last = bounce + 1 >= R.depth;
+            if (m.flags & kMatEmissive) {
+                float c[4] = {0.f, 0.f, 0.f, 0.f};
+                if (spectral) for (int k = 0; k < nch; k++) c[k] = tp[k] * emissive_at(m, lam[k]);
+                else { c[0] = tp[0] * m.emissive.x; c[1] = tp[1] * m.emissive.y; c[2] = tp[2] * m.emissive.z; }
+                const XyzWeights W = xyz_weights(spectral, lam, nch, wN, K.xyz_scale);
+                emit_xyz = apply_xyz(W, c);
+                emit = true;
+            } else if (m.flags & kMatMetallic) {
+                if (!last) {
+                    const float cosI = -f3dot(d, N);
+                    nd = f3add(d, f3mul(N, 2.f * cosI));
+                    no = f3add(hit, f3mul(N, 1e-3f));
+                    if (spectral) for (int k = 0; k < 4; k++) ntp[k] = tp[k] * albedo_at(m, lam[k]);
+                    else { ntp[0] = tp[0] * m.albedo.x; ntp[1] = tp[1] * m.albedo.y; ntp[2] = tp[2] * m.albedo.z; }
+                    cont = true;
+                }
+            } else if (m.flags & kMatTransparent) {
+                if (!last) {
+                    const float cosI = -f3dot(d, N);
+                    const bool disperse = spectral && m.cauchyB != 0.f && !single && nHero > 1;
+                    const int ways = disperse ? nHero : 1;
+                    const float4 coins = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 63u);
+                    for (int k = 0; k < ways; k++) {
+                        float ior = m.ior;
+                        if (spectral && m.cauchyB != 0.f && (disperse || single))
+                            ior = m.ior + m.cauchyB * 1e4f / (lam[k] * lam[k]);
+                        const float n1 = entering ? 1.f : ior, n2 = entering ? ior : 1.f;
+                        const float eta = n1 / n2;
+                        const float sinT2 = eta * eta * (1.f - cosI * cosI);
+                        const float u = k == 0 ? coins.x : (k == 1 ? coins.y : (k == 2 ? coins.z : coins.w));
+                        float3 bd, bo;
+                        bool refl = sinT2 >= 1.f;
+                        if (!refl) {
+                            float F0 = (n1 - n2) / (n1 + n2);
+                            F0 *= F0;
+                            const float F = F0 + (1.f - F0) * __powf(1.f - cosI, 5.f);
+                            refl = u < F;
+                        }
+                        if (refl) {
+                            bd = f3add(d, f3mul(N, 2.f * cosI));
+                            bo = f3add(hit, f3mul(N, 1e-3f));
+                        } else {
+                            const float cosT = sqrtf(1.f - sinT2);
+                            bd = f3add(f3mul(d, eta), f3mul(N, eta * cosI - cosT));
+                            bo = f3sub(hit, f3mul(N, 1e-3f));
+                        }
+                        if (disperse) {
+                            fork_o[k][0] = bo.x; fork_o[k][1] = bo.y; fork_o[k][2] = bo.z;
+                            fork_d[k][0] = bd.x; fork_d[k][1] = bd.y; fork_d[k][2] = bd.z;
+                            fork_tp[k] = tp[k] * albedo_at(m, lam[k]);
+                            fork_lam[k] = lam[k];
+                        } else {
+                            no = bo;
+                            nd = bd;
+                        }
+                    }
+                    if (disperse) {
+                        nfork = ways;
+                    } else {
+                        if (spectral) for (int k = 0; k < 4; k++) ntp[k] = tp[k] * albedo_at(m, lam[k]);
+                        else { ntp[0] = tp[0] * m.albedo.x; ntp[1] = tp[1] * m.albedo.y; ntp[2] = tp[2] * m.albedo.z; }
+                        cont = true;
+                    }
+                }
+            } else {
+                // diffuse
+                float al[4];
+                if (spectral) for (int k = 0; k < nch; k++) al[k] = albedo_at(m, lam[k]);
+                else { al[0] = m.albedo.x; al[1] = m.albedo.y; al[2] = m.albedo.z; }
+                // indirect origin: hit moved once by 1e-3*N (the reference's
+                // mutating `hit + N * 1e-3`, code/Renderer.cpp:782 with samples = 1)
+                float3 hc = f3add(hit, f3mul(N, 1e-3f));
+                const float3 h1 = hc;
+                if (S.total_light_area > 0.f) {
+                    const float invS = 1.f / (float)R.shadow;
+                    const XyzWeights W = xyz_weights(spectral, lam, nch, wN, K.xyz_scale);
+                    for (int s = 0; s < R.shadow; s++) {
+                        const float4 rr = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce,
+                                                1u + (uint32_t)s);
+                        int pick = 0;
+                        if (S.n_lights > 1) {
+                            const float target = rr.x * S.total_light_area;
+                            float cum = 0.f;
+                            for (int l = 0; l < S.n_lights; l++) {
+                                cum += S.lights[l].total_area;
+                                if (target <= cum) { pick = l; break; }
+                            }
+                        }
+                        const DLight& L = S.lights[pick];
+                        float3 P, Nl;
+                        int lm;
+                        if (L.kind == 0) {
+                            P = make_float3(L.o_mat.x + L.u.x * rr.y + L.v.x * rr.z, L.o_mat.y + L.u.y * rr.y + L.v.y * rr.z,
+                                            L.o_mat.z + L.u.z * rr.y + L.v.z * rr.z);
+                            Nl = xyz(L.n);
+                            lm = __float_as_int(L.o_mat.w);
+                        } else {
+                            const float4 r2 = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce,
+                                                    1000u + (uint32_t)s);
+                            const float rt = rr.y * L.total_area;
+                            const float* cum = S.light_cum + L.tri_offset;
+                            int lo = 0, hi = L.tri_count;
+                            while (lo < hi) { int mid = (lo + hi) >> 1; if (cum[mid] < rt) lo = mid + 1; else hi = mid; }
+                            const int ti = lo < L.tri_count - 1 ? lo : L.tri_count - 1;
+                            const DTri& lt = S.light_tris[L.tri_offset + ti];
+                            float a = rr.z, b = r2.x;
+                            if (a + b > 1.f) { a = 1.f - a; b = 1.f - b; }
+                            P = make_float3(lt.v0_id.x + lt.e1_mat.x * a + lt.e2_flags.x * b,
+                                            lt.v0_id.y + lt.e1_mat.y * a + lt.e2_flags.y * b,
+                                            lt.v0_id.z + lt.e1_mat.z * a + lt.e2_flags.z * b);
+                            Nl = xyz(S.light_flatn[L.tri_offset + ti]);
+                            lm = __float_as_int(lt.e1_mat.w);
+                        }
+                        const float3 Li = f3sub(P, hc);
+                        const float d2 = f3dot(Li, Li);
+                        const float3 wi = f3mul(Li, rsqrtf(d2));
+                        const float cosT = fmaxf(0.f, f3dot(wi, N));
+                        float3 so;
+                        // the lit-facing branch moves the shading point again
+                        // (code/Renderer.cpp:857, mutating operator+)
+                        if (cosT <= 0.f) so = f3sub(hc, f3mul(N, 1e-3f));
+                        else { hc = f3add(hc, f3mul(N, 1e-3f)); so = hc; }
+                        const float cosL = fmaxf(0.f, -f3dot(Nl, Li));
+                        const float G = (cosT * cosL) / d2;
+                        const bool useful = G > 0.f;
+                        float3 cx = make_float3(0.f, 0.f, 0.f);
+                        if (useful) {
+                            float w = 1.f;
+                            if ((R.flags & kReqMIS) && cosL > 1e-6f) {
+                                const float pL = d2 / (cosL * S.total_light_area), pB = cosT * inv_pi;
+                                w = (pL * pL) / (pL * pL + pB * pB);
+                            }
+                            const DMaterial& lmat = M[S.mat_base + lm];
+                            const float f = G * S.total_light_area * w * invS * inv_pi;
+                            float c[4] = {0.f, 0.f, 0.f, 0.f};
+                            if (spectral) for (int k = 0; k < nch; k++) c[k] = tp[k] * al[k] * emissive_at(lmat, lam[k]) * f;
+                            else {
+                                c[0] = tp[0] * al[0] * lmat.emissive.x * f;
+                                c[1] = tp[1] * al[1] * lmat.emissive.y * f;
+                                c[2] = tp[2] * al[2] * lmat.emissive.z * f;
+                            }
+                            cx = apply_xyz(W, c);
+                        }
+                        // append among the lanes that reach this point
+                        namespace cg = cooperative_groups;
+                        cg::coalesced_group g = cg::coalesced_threads();
+                        const int want = useful ? 1 : 0;
+                        const int ex = cg::exclusive_scan(g, want);
+                        const int tot = g.shfl(ex + want, g.size() - 1);
+                        int sbase = 0;
+                        if (g.thread_rank() == 0 && tot) sbase = atomicAdd(&C->shadow_n, tot);
+                        sbase = g.shfl(sbase, 0);
+                        if (useful) {
+                            const int pos = sbase + ex;
+                            if (pos < E.shadow_cap) {
+                                SQ.o[pos] = make_float4(so.x, so.y, so.z, d2);
+                                SQ.d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(id.y));
+                                SQ.c[pos] = make_float4(cx.x, cx.y, cx.z, __int_as_float(slot));
+                            } else {
+                                atomicOr(&C->status, 1);
+                            }
+                        }
+                    }
+                }
+                const float4 r0 = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 0u);
+                bool survive = !last;
+                float rr_scale = 1.f;
+                if (survive && (R.flags & kReqRussian) && bounce >= 1) {
+                    float pr = spectral ? al[0] : fmaxf(fmaxf(al[0], al[1]), al[2]);
+                    pr = fminf(0.95f, fmaxf(0.05f, pr));
+                    if (r0.w > pr) survive = false;
+                    else rr_scale = 1.f / pr;
+                }
+                if (survive) {
+                    float r1 = r0.x, r2 = r0.y;
+                    if ((R.flags & kReqStratified) && bounce == 0 && R.strata > 0) {
+                        const int sin_ = id.z % R.spp;
+                        const int sx = sin_ % R.strata, sy = (sin_ / R.strata) % R.strata;
+                        r1 = ((float)sx + r0.x) / (float)R.strata;
+                        r2 = ((float)sy + r0.y) / (float)R.strata;
+                    }
+                    nd = hemisphere(N, r1, r2);
+                    no = h1;
+                    for (int k = 0; k < 4; k++) ntp[k] = tp[k] * (k < (spectral ? nch : 3) ? al[k] : 0.f) * rr_scale;
+                    cont = true;
+                }
+            }
+        }
+
+        // ---- emit work (warp-uniform control flow from here)
+        if (emit) add_xyz(acc, emit_xyz);
+        const int newMeta = (bounce + 1) | (fork << 8) | (single << 11) | (nHero << 12);
+        {
+            int pos = warp_append(&C->queue_n[cur ^ 1], cont);
+            if (pos >= E.queue_cap) { atomicOr(&C->status, 2); pos = -1; }
+            if (pos >= 0) {
+                NQ.o[pos] = make_float4(no.x, no.y, no.z, o4.w);
+                NQ.d[pos] = make_float4(nd.x, nd.y, nd.z, __int_as_float(newMeta));
+                NQ.tp[pos] = make_float4(ntp[0], ntp[1], ntp[2], ntp[3]);
+                NQ.id[pos] = id;
+            }
+        }
+        for (int k = 0; k < 4; k++) {
+            int pos = warp_append(&C->queue_n[cur ^ 1], k < nfork);
+            if (pos >= E.queue_cap) { atomicOr(&C->status, 2); pos = -1; }
+            if (pos >= 0) {
+                const int fm = (bounce + 1) | ((k + 1) << 8) | (1 << 11) | (nHero << 12);
+                NQ.o[pos] = make_float4(fork_o[k][0], fork_o[k][1], fork_o[k][2], fork_lam[k]);
+                NQ.d[pos] = make_float4(fork_d[k][0], fork_d[k][1], fork_d[k][2], __int_as_float(fm));
+                NQ.tp[pos] = make_float4(fork_tp[k], fork_tp[k], fork_tp[k], fork_tp[k]);
+                NQ.id[pos] = id;
+            }
+            if (!__any_sync(0xffffffffu, k + 1 < nfork)) break;
+        }
+        // path bookkeeping: -1 for a retired path, +ways-1 for a fork
+        if (live) {
+            const long long delta = (cont ? 0 : -1) + (nfork > 0 ? nfork : 0);
+            if (delta != 0) atomicAdd((unsigned long long*)&E.outstanding[slot], (unsigned long long)delta);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ shadow
+// Shadow-ray test (code/Renderer.cpp:852-860): a closest-hit query bounded by
+// the light distance; the sample is blocked when the closest hit lies
+// closer than lightDist2 - 1e-3 (compared in double, as the reference's
+// double literal promotes it) and is not emissive.
+__global__ void k_shadow(EngineView E)
+{
+    Counters* C = E.cnt;
+    const int n = min(C->shadow_n, E.shadow_cap);
+    const ShadowQueue SQ = E.sq;
+    unsigned long long mine = 0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4 o = SQ.o[i], d = SQ.d[i], c = SQ.c[i];
+        const int slot = __float_as_int(c.w);
+        const DRequest& R = E.reqs[slot];
+        const DScene& S = E.scenes[R.scene];
+        const float d2 = o.w;
+        const float tmax = sqrtf(d2) * 1.0001f + 1e-4f;
+        float t = FLT_MAX, u, v;
+        const float3 so = xyz(o), wi = xyz(d);
+        const uint32_t prim = scene_closest(S, so, wi, tmax, t, u, v);
+        mine++;
+        bool lit = true;
+        if ((prim & kPrimKindMask) != kPrimNone) {
+            const float3 sh = make_float3(__fadd_rn(so.x, __fmul_rn(wi.x, t)), __fadd_rn(so.y, __fmul_rn(wi.y, t)),
+                                          __fadd_rn(so.z, __fmul_rn(wi.z, t)));
+            const float3 dd = ex::sub3(sh, so);
+            const float dist2 = ex::dot(dd, dd);
+            int mi;
+            const uint32_t kind = prim & kPrimKindMask, pidx = prim & kPrimIndexMask;
+            if (kind == kPrimSphere) mi = S.spheres[pidx].mat.x;
+            else if (kind == kPrimPlane) mi = __float_as_int(S.planes[pidx].o_mat.w);
+            else mi = __float_as_int(S.tris[pidx].e1_mat.w);
+            const bool em = (E.mats[S.mat_base + mi].flags & kMatEmissive) != 0;
+            if ((double)d2 - 1e-3 > (double)dist2 && !em) lit = false;
+        }
+        if (lit) add_xyz(R.accum + (size_t)__float_as_int(d.w) * 3, make_float3(c.x, c.y, c.z));
+    }
+    for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, off);
+    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&C->shadow_rays, mine);
+}
+
+// ------------------------------------------------------------------ status
+// End of iteration: marks requests whose paths are all issued and retired.
+__global__ void k_status(EngineView E, int next)
+{
+    Counters* C = E.cnt;
+    const int n_act = *E.n_active;
+    __shared__ int s_busy;
+    if (threadIdx.x == 0) s_busy = 0;
+    __syncthreads();
+    unsigned long long now;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(now));
+    for (int r = threadIdx.x; r < n_act; r += blockDim.x) {
+        const int slot = E.active[r];
+        if (E.done_flag[slot]) continue;
+        const bool all_issued = (long long)E.issued[slot] >= E.reqs[slot].total;
+        if (all_issued && E.outstanding[slot] == 0) {
+            E.done_flag[slot] = 1;
+            E.t_done[slot] = now;
+        } else {
+            s_busy = 1;
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        C->idle = (s_busy == 0 && C->queue_n[next] == 0) ? 1 : 0;
+        C->iter++;
+    }
+}
+
+// ------------------------------------------------------------------ resolve
+// Per-pixel mean -> linear sRGB (code/Renderer.cpp:300-302), then tone map
+// and 8-bit quantise (code/Renderer.cpp:365-382) on the device.
+__global__ void k_resolve(const double* __restrict__ acc, int npix, double inv_n, int spectral, int aces_tm,
+                          float* __restrict__ hdr, unsigned char* __restrict__ rgb8)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        float3 c = make_float3((float)(acc[i * 3] * inv_n), (float)(acc[i * 3 + 1] * inv_n), (float)(acc[i * 3 + 2] * inv_n));
+        if (spectral) c = xyz_to_srgb(c);
+        if (hdr) { hdr[i * 3] = c.x; hdr[i * 3 + 1] = c.y; hdr[i * 3 + 2] = c.z; }
+        if (rgb8) {
+            float3 m = aces_tm ? make_float3(aces(c.x), aces(c.y), aces(c.z)) : make_float3(reinhard(c.x), reinhard(c.y), reinhard(c.z));
+            rgb8[i * 3] = quantize(m.x);
+            rgb8[i * 3 + 1] = quantize(m.y);
+            rgb8[i * 3 + 2] = quantize(m.z);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ parity kernels
+__global__ void k_trace_rays(const DScene* scene, const DMaterial* mats, const float* __restrict__ rays, long long n,
+                             int* mat, int* prim_out, float* t_out, int bvh_only, int* counts)
+{
+    const DScene& S = *scene;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float3 o = make_float3(rays[i * 6], rays[i * 6 + 1], rays[i * 6 + 2]);
+        const float3 d = make_float3(rays[i * 6 + 3], rays[i * 6 + 4], rays[i * 6 + 5]);
+        float t = FLT_MAX, u = 0.f, v = 0.f;
+        if (bvh_only) {
+            TraceCounts tc = {0, 0};
+            int tri = counts ? bvh4_closest<true>(S, o, d, t, u, v, &tc) : bvh4_closest<false>(S, o, d, t, u, v, nullptr);
+            prim_out[i] = tri >= 0 ? __float_as_int(S.tris[tri].v0_id.w) : -1;
+            t_out[i] = tri >= 0 ? t : 0.f;
+            if (counts) { counts[i * 2] = tc.nodes; counts[i * 2 + 1] = tc.tris; }
+        } else {
+            const uint32_t prim = scene_closest(S, o, d, FLT_MAX, t, u, v);
+            const uint32_t kind = prim & kPrimKindMask, pidx = prim & kPrimIndexMask;
+            int mi = -1;
+            uint32_t code = 0;
+            if (kind == kPrimSphere) { mi = S.spheres[pidx].mat.x; code = kind | pidx; }
+            else if (kind == kPrimPlane) { mi = __float_as_int(S.planes[pidx].o_mat.w); code = kind | pidx; }
+            else if (kind == kPrimTri) {
+                mi = __float_as_int(S.tris[pidx].e1_mat.w);
+                code = kind | ((uint32_t)__float_as_int(S.tris[pidx].v0_id.w) & kPrimIndexMask);
+            }
+            mat[i] = mi;
+            prim_out[i] = (int)code;
+            t_out[i] = kind ? t : 0.f;
+        }
+    }
+}
+
+__global__ void k_eval_stage(int what, const float* __restrict__ params, const float* __restrict__ in, long long n,
+                             float* __restrict__ out, float xyz_scale)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        switch (what) {
+        case 0: out[i] = sigmoid_fit(make_float4(params[0], params[1], params[2], params[3]), in[i]); break;
+        case 1: out[i] = spectrum_lerp(params, in[i]); break;
+        case 2: { float3 c = cmf(in[i]); out[i * 3] = c.x; out[i * 3 + 1] = c.y; out[i * 3 + 2] = c.z; } break;
+        case 3: {
+            float3 c = cmf(in[i * 2]);
+            float r = in[i * 2 + 1];
+            out[i * 3] = r * c.x * xyz_scale; out[i * 3 + 1] = r * c.y * xyz_scale; out[i * 3 + 2] = r * c.z * xyz_scale;
+        } break;
+        case 4: { float3 c = xyz_to_srgb(make_float3(in[i * 3], in[i * 3 + 1], in[i * 3 + 2]));
+                  out[i * 3] = c.x; out[i * 3 + 1] = c.y; out[i * 3 + 2] = c.z; } break;
+        case 5: for (int k = 0; k < 3; k++) out[i * 3 + k] = reinhard(in[i * 3 + k]); break;
+        case 6: for (int k = 0; k < 3; k++) out[i * 3 + k] = aces(in[i * 3 + k]); break;
+        case 7: for (int k = 0; k < 3; k++) out[i * 3 + k] = (float)quantize(in[i * 3 + k]); break;
+        default: break;
+        }
+    }
+}
+
+}  // namespace pcr
