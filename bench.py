@@ -52,6 +52,10 @@ def args_():
     p.add_argument("--no-plain", action="store_true")
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-profile", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--queue", type=int, default=0, help="paths in flight (0: library default)")
+    p.add_argument("--serve-requests", type=int, default=400)
+    p.add_argument("--serve-rate", type=float, default=200.0)
     return p.parse_args()
 
 
@@ -148,7 +152,7 @@ def reference_arm(a):
     files, data = scene_files()
     scenes = {v: ref.load_scene(os.path.abspath(p), data) for v, p in files.items()}
     batch = make_batch(a.renders, a.seed)
-    rows = 2
+    rows = os.cpu_count() or 8   # one row per host thread
     for _ in range(a.warmup):
         cpu_sample_step(scenes, batch, rows)
     tot_p, tot_s = 0, 0.0
@@ -166,6 +170,45 @@ def reference_arm(a):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"{rows} rows of each of the {a.renders} renders per step"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ------------------------------------------------------------------ served stream
+def serve_run(ctx, sids, files, data, a):
+    """Requests arrive by a Poisson process at `rate` req/s (scene drawn from
+    the 10 variants, 20 % the seeded ~70k-triangle mesh scene, glass or
+    Lambertian by seed; square resolution log-uniform 64..1024, depth 2..8,
+    paths per pixel 1..64, shadow rays 1..8).  The engine serves them on its
+    own thread; a request is admitted as slots and the device-memory budget
+    free up, and its paths share the queue with everything in flight.
+    Latency is submit -> result on the host, per request."""
+    from pcr_b200 import capi, workloads
+    mesh = {False: ctx.load_scene_json(workloads.mesh_scene(59, 11, glass=False), data),
+            True: ctx.load_scene_json(workloads.mesh_scene(59, 12, glass=True), data)}
+    reqs = workloads.request_stream(a.serve_requests, a.serve_rate, seed=a.seed + 17)
+    ctx.serve_start()
+    t0 = time.perf_counter()
+    ids = []
+    for r in reqs:
+        now = time.perf_counter() - t0
+        if r["arrival"] > now:
+            time.sleep(r["arrival"] - now)
+        sid = mesh[bool(r["seed"] & 1)] if r["variant"] == "mesh" else sids[r["variant"]]
+        d = capi.render_desc(r["width"], r["height"], depth=r["depth"], samples=r["samples"], shadow=r["shadow"],
+                             spectral=True, seed=r["seed"])
+        ids.append((ctx.submit(sid, d), r))
+    lat, paths, t_last = [], 0, 0.0
+    for rid, r in ids:
+        ctx.wait(rid, 600_000)
+        _, _, st = ctx.fetch(rid, want_hdr=False, want_rgb=False)
+        lat.append(st.latency_ms)
+        paths += st.paths
+        t_last = max(t_last, r["arrival"] * 1e3 + st.latency_ms)
+    ctx.serve_stop()
+    lat = np.asarray(lat)
+    return {"requests": len(ids), "rate_req_s": a.serve_rate, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
+            "paths_per_s": paths / (t_last / 1e3), "span_s": t_last / 1e3,
+            "mesh_fraction": 0.2, "resolution": "log-uniform 64..1024"}
 
 
 # ------------------------------------------------------------------ CUDA arm
@@ -189,7 +232,7 @@ def main():
 
     from pcr_b200 import capi
     torch.cuda.set_device(local)
-    ctx = capi.Context(device=local)
+    ctx = capi.Context(device=local, queue_capacity=a.queue)
     stream = torch.cuda.ExternalStream(ctx.stream())
     files, data = scene_files()
     sids = {v: ctx.load_scene_json(p, data) for v, p in files.items()}
@@ -244,13 +287,15 @@ def main():
     rays = sum_over_ranks(st["rays"] + st["shadow_rays"]) / (ms / 1e3)
 
     # ---- e2e: host buffers in and out through the C ABI, host clock
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(a.steps):
-        batched_step(want_images=True)
-    barrier()
-    e2e_s = max_over_ranks(time.perf_counter() - t0)
-    e2e = total_paths / e2e_s
+    e2e = None
+    if not a.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(a.steps):
+            batched_step(want_images=True)
+        barrier()
+        e2e_s = max_over_ranks(time.perf_counter() - t0)
+        e2e = total_paths / e2e_s
     d2h = sum(r["width"] * r["height"] * 15 for r in batch)
     h2d = a.renders * 96
 
@@ -270,7 +315,7 @@ def main():
     # ---- per-stage events (profiled pass) for the roofline
     roofline = None
     if not a.no_profile:
-        pctx = capi.Context(device=local, profile=True)
+        pctx = capi.Context(device=local, profile=True, queue_capacity=a.queue)
         psids = {v: pctx.load_scene_json(p, data) for v, p in files.items()}
         ids = [pctx.submit(psids[r["variant"]], d) for r, d in zip(batch, descs)]
         pctx.run_until_idle()
@@ -295,6 +340,11 @@ def main():
                     "stage_ms": ps["stage_ms"], "stage_share": {k: v / max(1e-9, sum(ps["stage_ms"].values()))
                                                                 for k, v in ps["stage_ms"].items()}}
 
+    # ---- served stream: Poisson arrivals, continuous batching, p50/p99
+    serve = None
+    if a.serve_requests > 0:
+        serve = serve_run(ctx, sids, files, data, a)
+
     # ---- CPU baseline (rank 0, N = 1): reference renderer on a row sample
     cpu = None
     if not a.no_cpu and rank == 0 and world == 1:
@@ -302,9 +352,10 @@ def main():
             from oracle import ref
             if ref.available():
                 rscenes = {v: ref.load_scene(os.path.abspath(p), data) for v, p in files.items()}
-                pp, ss = cpu_sample_step(rscenes, batch, 2)
+                rows = os.cpu_count() or 8   # one row per host thread
+                pp, ss = cpu_sample_step(rscenes, batch, rows)
                 cpu = {"value": pp / ss, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                       "sample": f"2 pixel rows of each of the {a.renders} renders ({pp} paths, {ss:.1f} s)"}
+                       "sample": f"{rows} pixel rows of each of the {a.renders} renders ({pp} paths, {ss:.1f} s)"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)}
 
@@ -323,6 +374,7 @@ def main():
             "plain_value": plain, "batched_over_plain": (value / plain) if plain else None,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+            "serve": serve,
             "tuning": {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")},
         }
         print(json.dumps(out))

@@ -84,7 +84,8 @@ class SceneDesc(C.Structure):
 class RenderDesc(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "width", "height", "depth", "samples", "shadow_samples", "spectral", "hero_samples", "mis", "russian",
-        "stratified", "aa_samples", "adaptive", "aces", "denoise")] + [("seed", C.c_uint64), ("priority", C.c_int32)]
+        "stratified", "aa_samples", "adaptive", "aces", "denoise")] + [("seed", C.c_uint64), ("priority", C.c_int32),
+                                                                ("multi_sample", C.c_int32)]
 
 
 class RenderStats(C.Structure):
@@ -175,9 +176,10 @@ def _ip(a):
 
 def render_desc(width, height=None, depth=4, samples=16, shadow=4, spectral=True, hero=4, mis=False,
                 russian=False, stratified=False, aa=1, adaptive=False, aces=False, denoise=False, seed=1,
-                priority=0) -> RenderDesc:
+                priority=0, multi_sample=False) -> RenderDesc:
     return RenderDesc(width, height or width, depth, samples, shadow, int(spectral), hero, int(mis),
-                      int(russian), int(stratified), aa, int(adaptive), int(aces), int(denoise), seed, priority)
+                      int(russian), int(stratified), aa, int(adaptive), int(aces), int(denoise), seed, priority,
+                      int(multi_sample))
 
 
 class HostScene:

@@ -1,0 +1,270 @@
+// CudaRenderer: see cuda_renderer.h.
+#include "cuda_renderer.h"
+
+#include <zlib.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <ctime>
+#include <filesystem>
+#include <iostream>
+#include <random>
+
+namespace pcr {
+
+// ------------------------------------------------------------------ bilateral
+void bilateral_rgb(std::vector<uint8_t>& rgb, int width, int height)
+{
+    // 5x5 cross-bilateral, two passes (code/Denoise.cpp:14-86)
+    if (width <= 0 || height <= 0 || rgb.size() < (size_t)width * height * 3) return;
+    const int radius = 2;
+    const float invSpatial2 = 1.0f / (2.0f * 1.5f * 1.5f);
+    const float invColor2 = 1.0f / (2.0f * 10.0f * 10.0f);
+    std::vector<uint8_t> out(rgb.size());
+    for (int pass = 0; pass < 2; pass++) {
+        const std::vector<uint8_t>& src = pass == 0 ? rgb : out;
+        std::vector<uint8_t>& dst = pass == 0 ? out : rgb;
+        for (int y = 0; y < height; y++)
+            for (int x = 0; x < width; x++) {
+                const size_t c = ((size_t)y * width + x) * 3;
+                const float cR = src[c], cG = src[c + 1], cB = src[c + 2];
+                float sw = 0.f, sr = 0.f, sg = 0.f, sb = 0.f;
+                for (int dy = -radius; dy <= radius; dy++) {
+                    const int ny = y + dy;
+                    if (ny < 0 || ny >= height) continue;
+                    for (int dx = -radius; dx <= radius; dx++) {
+                        const int nx = x + dx;
+                        if (nx < 0 || nx >= width) continue;
+                        const size_t n = ((size_t)ny * width + nx) * 3;
+                        const float nR = src[n], nG = src[n + 1], nB = src[n + 2];
+                        const float sp = (float)(dx * dx + dy * dy) * invSpatial2;
+                        const float dR = nR - cR, dG = nG - cG, dB = nB - cB;
+                        const float col = (dR * dR + dG * dG + dB * dB) * invColor2;
+                        const float w = std::exp(-(sp + col));
+                        sw += w;
+                        sr += w * nR;
+                        sg += w * nG;
+                        sb += w * nB;
+                    }
+                }
+                if (sw > 0.0f) {
+                    dst[c] = (uint8_t)std::min(255.0f, sr / sw + 0.5f);
+                    dst[c + 1] = (uint8_t)std::min(255.0f, sg / sw + 0.5f);
+                    dst[c + 2] = (uint8_t)std::min(255.0f, sb / sw + 0.5f);
+                } else {
+                    dst[c] = src[c];
+                    dst[c + 1] = src[c + 1];
+                    dst[c + 2] = src[c + 2];
+                }
+            }
+    }
+}
+
+// ------------------------------------------------------------------ PNG
+namespace {
+void put32(std::vector<uint8_t>& o, uint32_t v)
+{
+    o.push_back((uint8_t)(v >> 24));
+    o.push_back((uint8_t)(v >> 16));
+    o.push_back((uint8_t)(v >> 8));
+    o.push_back((uint8_t)v);
+}
+void chunk(std::vector<uint8_t>& o, const char* type, const std::vector<uint8_t>& data)
+{
+    put32(o, (uint32_t)data.size());
+    size_t start = o.size();
+    o.insert(o.end(), type, type + 4);
+    o.insert(o.end(), data.begin(), data.end());
+    uLong crc = crc32(0L, Z_NULL, 0);
+    crc = crc32(crc, o.data() + start, (uInt)(o.size() - start));
+    put32(o, (uint32_t)crc);
+}
+
+std::string compress_zone(const std::string& z)
+{
+    // strftime("%Z") gives long names on some platforms; keep the short
+    // POSIX form (code/Renderer.cpp:37-74)
+    if (z.find(' ') == std::string::npos) return z;
+    std::string a;
+    bool start = true;
+    for (char c : z) {
+        if (c == ' ') { start = true; continue; }
+        if (start && std::isalpha((unsigned char)c)) a += (char)std::toupper((unsigned char)c);
+        start = false;
+    }
+    return a.empty() ? z : a;
+}
+
+std::string timestamp()
+{
+    // "YYYYMMDD-HHMMSS-<ZONE>", local time (code/Renderer.cpp:79-105)
+    std::time_t now = std::time(nullptr);
+    std::tm tm{};
+    localtime_r(&now, &tm);
+    char buf[64], zone[64];
+    std::strftime(buf, sizeof(buf), "%Y%m%d-%H%M%S", &tm);
+    std::strftime(zone, sizeof(zone), "%Z", &tm);
+    return std::string(buf) + "-" + compress_zone(zone);
+}
+}  // namespace
+
+bool write_png(const std::string& path, const uint8_t* rgb, int width, int height,
+               const std::vector<std::pair<std::string, std::string>>& text)
+{
+    std::vector<uint8_t> o = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
+    std::vector<uint8_t> ihdr;
+    put32(ihdr, (uint32_t)width);
+    put32(ihdr, (uint32_t)height);
+    ihdr.insert(ihdr.end(), {8, 2, 0, 0, 0});  // 8-bit RGB
+    chunk(o, "IHDR", ihdr);
+    for (const auto& kv : text) {  // tEXt ahead of IDAT
+        std::vector<uint8_t> t(kv.first.begin(), kv.first.end());
+        t.push_back(0);
+        t.insert(t.end(), kv.second.begin(), kv.second.end());
+        chunk(o, "tEXt", t);
+    }
+    std::vector<uint8_t> raw((size_t)(width * 3 + 1) * height);
+    for (int y = 0; y < height; y++) {
+        raw[(size_t)y * (width * 3 + 1)] = 0;
+        std::memcpy(&raw[(size_t)y * (width * 3 + 1) + 1], rgb + (size_t)y * width * 3, (size_t)width * 3);
+    }
+    uLongf zlen = compressBound((uLong)raw.size());
+    std::vector<uint8_t> z(zlen);
+    if (compress2(z.data(), &zlen, raw.data(), (uLong)raw.size(), 6) != Z_OK) return false;
+    z.resize(zlen);
+    chunk(o, "IDAT", z);
+    chunk(o, "IEND", {});
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return false;
+    bool ok = std::fwrite(o.data(), 1, o.size(), f) == o.size();
+    ok = std::fclose(f) == 0 && ok;
+    return ok;
+}
+
+// ------------------------------------------------------------------ renderer
+CudaRenderer::CudaRenderer(int width, int height, int depth, int samples, int shadowSamples, GLFWwindow*)
+    : _width(width), _height(height), _maxDepth(depth), _samples(samples), _shadowSamples(shadowSamples)
+{
+}
+
+CudaRenderer::~CudaRenderer()
+{
+    if (_ctx) pcr_ctx_destroy(_ctx);
+}
+
+pcr_render_desc CudaRenderer::desc() const
+{
+    pcr_render_desc d{};
+    d.width = _width;
+    d.height = _height;
+    d.depth = _maxDepth;
+    d.samples = _samples;
+    d.shadow_samples = _shadowSamples;
+    d.spectral = useSpectral;
+    d.hero_samples = heroSamples;
+    d.mis = useMIS;
+    d.russian = useRussian;
+    d.stratified = useStratified;
+    d.aa_samples = std::max(1, aaSamples);
+    d.adaptive = useAdaptive;
+    d.aces = useACES;
+    d.denoise = useDenoise;
+    d.multi_sample = wavefrontMultiSample;
+    d.seed = seed ? seed : (uint64_t)std::random_device{}() << 32 | std::random_device{}();
+    return d;
+}
+
+bool CudaRenderer::render_to(const pcr_scene_desc& scene, RenderOutput& out)
+{
+    if (!_ctx) {
+        pcr_ctx_opts o{};
+        const char* dev = std::getenv("PCR_DEVICE");
+        o.device = dev ? std::atoi(dev) : 0;
+        o.use_graph = 1;
+        if (pcr_ctx_create(&_ctx, &o) != PCR_OK) {
+            std::cerr << "pcr: " << pcr_last_error() << std::endl;
+            _ctx = nullptr;
+            return false;
+        }
+    }
+    const void* key = scene.materials;
+    if (_scene < 0 || key != _scene_key) {
+        if (_scene >= 0) pcr_scene_release(_ctx, _scene);
+        _scene = -1;
+        if (pcr_scene_upload(_ctx, &scene, &_scene) != PCR_OK) {
+            std::cerr << "pcr: scene upload failed: " << pcr_last_error() << std::endl;
+            return false;
+        }
+        _scene_key = key;
+    }
+    if (useAdaptive)
+        std::cerr << "warning: --adaptive is not applied by the CUDA backend; rendering all aa samples.\n";
+    pcr_render_desc d = desc();
+    out.hdr.assign((size_t)_width * _height * 3, 0.f);
+    out.rgb8.assign((size_t)_width * _height * 3, 0);
+    pcr_render_stats st{};
+    if (pcr_render(_ctx, _scene, &d, out.hdr.data(), out.rgb8.data(), &st) != PCR_OK) {
+        std::cerr << "pcr: render failed: " << pcr_last_error() << std::endl;
+        return false;
+    }
+    if (useOIDN)
+        std::cerr << "warning: --oidn requested but binary was not built with PCR_USE_OIDN=ON; skipping denoise.\n";
+    if (useDenoise) bilateral_rgb(out.rgb8, _width, _height);
+    if (progressRows) progressRows->store(_height, std::memory_order_relaxed);
+    if (onPartialFrame) {
+        std::vector<std::array<float, 3>> fb((size_t)_width * _height);
+        for (size_t i = 0; i < fb.size(); i++) fb[i] = {out.hdr[i * 3], out.hdr[i * 3 + 1], out.hdr[i * 3 + 2]};
+        onPartialFrame(fb, _width, _height);
+    }
+    return true;
+}
+
+void CudaRenderer::render(const pcr_scene_desc& scene, std::chrono::steady_clock::time_point start,
+                          const std::string& outputDir)
+{
+    lastOutputPath.clear();
+    if (cancelRequested && cancelRequested->load(std::memory_order_relaxed)) {
+        std::cout << "Render cancelled before write." << std::endl;
+        return;
+    }
+    RenderOutput out;
+    if (!render_to(scene, out)) return;
+    if (cancelRequested && cancelRequested->load(std::memory_order_relaxed)) {
+        std::cout << "Render cancelled before write." << std::endl;
+        return;
+    }
+    auto ms = std::chrono::duration_cast<std::chrono::milliseconds>(std::chrono::steady_clock::now() - start).count();
+    std::cout << "Render took " << ms << " ms" << std::endl;
+    const std::string ts = timestamp();
+    std::string name = std::string(scene.name ? scene.name : "scene") + "-" + (scene.version ? scene.version : "") +
+                       "-" + ts + "-d" + std::to_string(_maxDepth) + "-s" + std::to_string(_samples) + "-S" +
+                       std::to_string(_shadowSamples) + "-w" + std::to_string(_width);
+    if (_width != _height) name += "-h" + std::to_string(_height);
+    if (useSpectral) name += "-spectral";
+    if (useACES) name += "-aces";
+    name += "-t" + std::to_string(ms) + ".png";
+    std::filesystem::path p = std::filesystem::path(outputDir) / name;
+    std::error_code ec;
+    std::filesystem::create_directories(p.parent_path(), ec);
+    // tEXt keys of code/Renderer.cpp:429-447
+    std::vector<std::pair<std::string, std::string>> text = {
+        {"Software", binaryName}, {"Scene", scene.name ? scene.name : ""},
+        {"SceneVersion", scene.version ? scene.version : ""}, {"CreationTime", ts},
+        {"Depth", std::to_string(_maxDepth)}, {"Samples", std::to_string(_samples)},
+        {"ShadowSamples", std::to_string(_shadowSamples)}, {"Width", std::to_string(_width)},
+        {"Height", std::to_string(_height)}, {"RenderTimeMs", std::to_string(ms)},
+        {"Denoise", useDenoise ? "1" : "0"}, {"MIS", useMIS ? "1" : "0"}, {"Russian", useRussian ? "1" : "0"},
+        {"Stratified", useStratified ? "1" : "0"}, {"Tonemap", useACES ? "ACES" : "Reinhard"},
+        {"AASamples", std::to_string(aaSamples)}, {"Adaptive", useAdaptive ? "1" : "0"},
+        {"OIDN", useOIDN ? "1" : "0"}, {"Spectral", useSpectral ? "1" : "0"}};
+    if (!write_png(p.string(), out.rgb8.data(), _width, _height, text)) {
+        std::cerr << "png save error (path: " << p << ")" << std::endl;
+        return;
+    }
+    std::cout << "Wrote " << p << std::endl;
+    lastOutputPath = p.string();
+}
+
+}  // namespace pcr

@@ -67,22 +67,43 @@ __device__ __forceinline__ bool sphere_hit(const DSphere& s, float3 o, float3 d,
 
 // Plane::intersect (code/Includes/Plane.h:33-54); uu, vv precomputed with
 // the same dot the reference evaluates per call.
+//
+// The three IEEE divides are first decided by a reciprocal product: for
+// x > 0, y > 0 normal, x * rcp(y) is within 2^-23 relative of x / y, so a
+// product beyond a bound by 2^-20 fixes the comparison the correctly rounded
+// quotient would make.  Only the t of planes that survive, and quotients near
+// a bound, are divided exactly; the accept/reject decisions and t are the
+// same as dividing every time.  t0 is only meaningful when true is returned.
 __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, float closest, float& t0)
 {
     using namespace ex;
+    const float kUp = 1.f + 9.5367431640625e-07f, kDown = 1.f - 9.5367431640625e-07f;  // 1 +- 2^-20
     float4 nA = p.n_area;
     float3 N = make_float3(nA.x, nA.y, nA.z);
     float denom = dot(d, N);
     if (fabsf(denom) <= 1e-6f) return false;
     float4 oM = p.o_mat;
     float3 po = make_float3(oM.x, oM.y, oM.z);
-    float t = div(dot(sub3(po, o), N), denom);
+    float num = dot(sub3(po, o), N);
+    // t = num / denom is <= 0 when the signs differ (or num is zero)
+    const float an = denom > 0.f ? num : -num;
+    if (an <= 0.f) return false;
+    const float tq = an * __frcp_rn(fabsf(denom));
+    if (tq > closest * kUp || tq < 1e-6f * kDown) return false;
+    float t = div(num, denom);
     t0 = t;
     if (t <= 1e-6f || t > closest) return false;
     float3 lh = sub3(add3(o, scale3(d, t)), po);
     float4 u = p.u_uu, v = p.v_vv;
-    float s = div(dot(lh, make_float3(u.x, u.y, u.z)), u.w);
-    float q = div(dot(lh, make_float3(v.x, v.y, v.z)), v.w);
+    float a = dot(lh, make_float3(u.x, u.y, u.z));
+    float b = dot(lh, make_float3(v.x, v.y, v.z));
+    // s = a / uu, q = b / vv must lie in [0, 1]; uu, vv > 0.  a < -1e-20
+    // makes s negative (|a / uu| stays far above the smallest subnormal for
+    // any |u| < 1e12).
+    if (a < -1e-20f || b < -1e-20f) return false;
+    if (a * __frcp_rn(u.w) > kUp || b * __frcp_rn(v.w) > kUp) return false;
+    float s = div(a, u.w);
+    float q = div(b, v.w);
     if (s > 1.f || s < 0.f || q > 1.f || q < 0.f) return false;
     return true;
 }
@@ -273,7 +294,11 @@ __device__ __forceinline__ float wyman(float l, float mu, float s1, float s2)
 {
     using namespace ex;
     float t = (l < mu) ? mul(sub(l, mu), s1) : mul(sub(l, mu), s2);
-    return expf(mul(mul(-0.5f, t), t));
+    // the exponential is taken in double and rounded once, which gives the
+    // correctly rounded float result; x-bar's negative lobe cancels against
+    // the other two near 500 nm, so a float exp's last-bit error would be
+    // amplified past 1e-5 there
+    return (float)exp((double)mul(mul(-0.5f, t), t));
 }
 __device__ __forceinline__ float3 cmf(float l)
 {

@@ -99,6 +99,7 @@ Engine::Engine(const pcr_ctx_opts* o)
     CK(cudaSetDevice(device_));
     CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     xyz_scale_ = (700.f - 400.f) / host_ybar_integral();
     slot_owner_.assign(kMaxActive, -1);
     scenes_.reserve(256);
@@ -120,10 +121,10 @@ Engine::~Engine()
         if (r.accum) cudaFree(r.accum);
         if (r.d_hdr) cudaFree(r.d_hdr);
         if (r.d_rgb) cudaFree(r.d_rgb);
-        if (r.h_hdr) cudaFreeHost(r.h_hdr);
-        if (r.h_rgb) cudaFreeHost(r.h_rgb);
         if (r.ev_ready) cudaEventDestroy(r.ev_ready);
     }
+    if (staging_) cudaFreeHost(staging_);
+    cudaStreamDestroy(copy_stream_);
     for (auto& s : scenes_)
         for (void* p : s.allocs) cudaFree(p);
     free_buffers();
@@ -682,19 +683,40 @@ void Engine::finish_request(Request& r)
     k_resolve<<<std::max(1, grid), 256, 0, stream_>>>(r.accum, (int)px, inv, d.spectral ? 1 : 0, d.aces ? 1 : 0,
                                                        r.d_hdr, r.d_rgb);
     CK(cudaGetLastError());
-    if (!r.h_hdr) CK(cudaMallocHost(&r.h_hdr, px * 3 * sizeof(float)));
-    if (!r.h_rgb) CK(cudaMallocHost(&r.h_rgb, px * 3));
-    CK(cudaMemcpyAsync(r.h_hdr, r.d_hdr, px * 3 * sizeof(float), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(r.h_rgb, r.d_rgb, px * 3, cudaMemcpyDeviceToHost, stream_));
+    // the resolved images stay on the device until fetch copies them out
     CK(cudaFreeAsync(r.accum, stream_));
-    CK(cudaFreeAsync(r.d_hdr, stream_));
-    CK(cudaFreeAsync(r.d_rgb, stream_));
     r.accum = nullptr;
-    r.d_hdr = nullptr;
-    r.d_rgb = nullptr;
     if (!r.ev_ready) CK(cudaEventCreateWithFlags(&r.ev_ready, cudaEventDisableTiming));
     CK(cudaEventRecord(r.ev_ready, stream_));
     r.state = ReqState::Resolving;
+}
+
+// Copies a resolved request's images to caller host buffers through one
+// reusable pinned staging buffer on the copy stream (ordered after the
+// resolve by the request's event), then frees its device images.
+void Engine::copy_out(Request& r, float* hdr, uint8_t* rgb)
+{
+    std::lock_guard<std::mutex> g(copy_mu_);
+    const int64_t px = (int64_t)r.desc.width * r.desc.height;
+    const size_t need = (size_t)px * 3 * (sizeof(float) + 1);
+    if ((hdr || rgb) && need > staging_bytes_) {
+        if (staging_) CK(cudaFreeHost(staging_));
+        staging_ = nullptr;
+        CK(cudaMallocHost(&staging_, need));
+        staging_bytes_ = need;
+    }
+    CK(cudaStreamWaitEvent(copy_stream_, r.ev_ready, 0));
+    float* sh = reinterpret_cast<float*>(staging_);
+    uint8_t* sr = staging_ ? staging_ + px * 3 * sizeof(float) : nullptr;
+    if (hdr) CK(cudaMemcpyAsync(sh, r.d_hdr, px * 3 * sizeof(float), cudaMemcpyDeviceToHost, copy_stream_));
+    if (rgb) CK(cudaMemcpyAsync(sr, r.d_rgb, px * 3, cudaMemcpyDeviceToHost, copy_stream_));
+    CK(cudaFreeAsync(r.d_hdr, copy_stream_));
+    CK(cudaFreeAsync(r.d_rgb, copy_stream_));
+    r.d_hdr = nullptr;
+    r.d_rgb = nullptr;
+    CK(cudaStreamSynchronize(copy_stream_));
+    if (hdr) std::memcpy(hdr, sh, px * 3 * sizeof(float));
+    if (rgb) std::memcpy(rgb, sr, px * 3);
 }
 
 void Engine::harvest(bool)
@@ -858,11 +880,15 @@ void Engine::wait(int64_t id, int64_t timeout_ms)
 void Engine::fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st)
 {
     if (!poll(id)) throw PcrError(PCR_ERR_INVALID, "request not finished");
-    std::lock_guard<std::mutex> g(mu_);
-    Request& r = *reqs_[id];
-    const int64_t px = (int64_t)r.desc.width * r.desc.height;
-    if (hdr) std::memcpy(hdr, r.h_hdr, px * 3 * sizeof(float));
-    if (rgb) std::memcpy(rgb, r.h_rgb, px * 3);
+    std::unique_ptr<Request> owned;
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = reqs_.find(id);
+        owned = std::move(it->second);
+        reqs_.erase(it);
+    }
+    Request& r = *owned;
+    copy_out(r, hdr, rgb);
     if (st) {
         st->device_ms = r.device_ms;
         st->latency_ms = std::chrono::duration<double, std::milli>(r.t_ready - r.t_submit).count();
@@ -871,10 +897,7 @@ void Engine::fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st)
         st->rays = 0;
         st->shadow_rays = 0;
     }
-    if (r.h_hdr) cudaFreeHost(r.h_hdr);
-    if (r.h_rgb) cudaFreeHost(r.h_rgb);
     if (r.ev_ready) cudaEventDestroy(r.ev_ready);
-    reqs_.erase(id);
 }
 
 void Engine::cancel(int64_t id)
@@ -904,13 +927,17 @@ void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, ui
     r.bytes = request_bytes(desc);
     if (r.bytes > budget_) throw PcrError(PCR_ERR_NO_MEMORY, "request larger than the device memory budget");
     if (graph_dirty_) build_graph();
-    EngineParams p{tune_.queue_capacity, tune_.queue_capacity, 1, 1};
+    // a pass holds one sample per pixel (W*H paths) unless multi_sample asks
+    // for passes as large as the queue; no refill until a pass has drained
+    const int64_t px = (int64_t)desc.width * desc.height;
+    const int pass = desc.multi_sample ? tune_.queue_capacity : (int)std::min<int64_t>(px, tune_.queue_capacity);
+    EngineParams p{pass, pass, 1, 1};
     k_set_params<<<1, 1, 0, stream_>>>((EngineParams*)d_params_, p);
     activate(r, 0);
     slot_owner_[0] = -1;  // the plain request is not in the request map
     upload_active();
-    const int64_t total = (int64_t)desc.width * desc.height * desc.samples * std::max(1, desc.aa_samples);
-    const int64_t passes = (total + tune_.queue_capacity - 1) / tune_.queue_capacity;
+    const int64_t total = px * desc.samples * std::max(1, desc.aa_samples);
+    const int64_t passes = (total + pass - 1) / pass;
     int cur = 0;
     for (int64_t it = 0; it < passes * (int64_t)desc.depth; it++) {
         launch_iteration(cur, profile_);
@@ -938,19 +965,13 @@ void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, ui
     CK(cudaMemcpy(&tf, d_tfirst_, 8, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&td, d_tdone_, 8, cudaMemcpyDeviceToHost));
     finish_request(r);
-    CK(cudaStreamSynchronize(stream_));
     active_slots_.clear();
     active_dirty_ = true;
     bytes_in_use_ -= r.bytes;
     upload_active();
     EngineParams q{tune_.queue_capacity, tune_.chunk_paths, tune_.regen_every, 0};
     k_set_params<<<1, 1, 0, stream_>>>((EngineParams*)d_params_, q);
-    CK(cudaStreamSynchronize(stream_));
-    const int64_t px = (int64_t)desc.width * desc.height;
-    if (hdr) std::memcpy(hdr, r.h_hdr, px * 3 * sizeof(float));
-    if (rgb) std::memcpy(rgb, r.h_rgb, px * 3);
-    cudaFreeHost(r.h_hdr);
-    cudaFreeHost(r.h_rgb);
+    copy_out(r, hdr, rgb);
     cudaEventDestroy(r.ev_ready);
     if (st) {
         st->device_ms = (td > tf && tf) ? (double)(td - tf) * 1e-6 : 0.0;

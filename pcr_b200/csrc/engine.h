@@ -48,8 +48,6 @@ struct Request {
     double* accum = nullptr;
     float* d_hdr = nullptr;
     uint8_t* d_rgb = nullptr;
-    float* h_hdr = nullptr;      // pinned
-    uint8_t* h_rgb = nullptr;    // pinned
     cudaEvent_t ev_ready = nullptr;
     std::chrono::steady_clock::time_point t_submit, t_admit, t_ready;
     double device_ms = 0;
@@ -108,6 +106,7 @@ private:
     void build_graph();
     void harvest(bool final_sync);
     void finish_request(Request& r);
+    void copy_out(Request& r, float* hdr, uint8_t* rgb);
     void check_status();
     bool engine_step();
     void serve_loop();
@@ -117,6 +116,10 @@ private:
     int device_ = 0;
     int sms_ = 148;
     cudaStream_t stream_ = nullptr;
+    cudaStream_t copy_stream_ = nullptr;   // result copies, ordered by request events
+    std::mutex copy_mu_;
+    uint8_t* staging_ = nullptr;           // pinned, reused across fetches
+    size_t staging_bytes_ = 0;
     EngineTuning tune_;
     bool use_graph_ = true, profile_ = false;
     int64_t budget_ = 40ll << 30;

@@ -204,7 +204,9 @@ __device__ __forceinline__ void add_xyz(double* acc, float3 c)
 struct XyzWeights {
     float3 w[4];
 };
-__device__ __forceinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale)
+// Kept out of line: seven double-precision exponentials per wavelength make
+// a large body, and one shared copy keeps k_shade's instruction footprint small.
+__device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale)
 {
     XyzWeights W;
     if (!spectral) {
@@ -241,12 +243,31 @@ struct ShadeConst {
 };
 
 // ------------------------------------------------------------------ shade
+// Appends `count` records for the calling lane among the lanes that reach the
+// call together (divergent code): one atomic per coalesced group.
+__device__ __forceinline__ int group_append(int* counter, int count)
+{
+    namespace cg = cooperative_groups;
+    cg::coalesced_group g = cg::coalesced_threads();
+    const int ex = cg::exclusive_scan(g, count);
+    const int tot = g.shfl(ex + count, g.size() - 1);
+    int base = 0;
+    if (g.thread_rank() == 0 && tot) base = atomicAdd(counter, tot);
+    return g.shfl(base, 0) + ex;
+}
+
 // Per-path shading of the hit found by k_extend (code/Renderer.cpp:656-889
 // with samples = 1, the GPU's paths-per-pixel estimator): emission,
 // mirror, dielectric (with the 4-way hero fork at dispersive glass),
 // diffuse direct lighting via explicit shadow rays, Russian roulette and the
 // cosine-hemisphere continuation.  Materials are staged in shared memory.
-__global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
+//
+// A diffuse vertex reserves R.shadow shadow records with one append; samples
+// whose geometry term is zero are written as skip records (lightDist2 < 0).
+// The spectral product albedo * emission * XYZ weight is formed once per
+// vertex and light material, so each shadow sample only scales it by its
+// geometry term.
+__global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
 {
     extern __shared__ DMaterial s_mat[];
     const DMaterial* M = E.mats;
@@ -264,6 +285,7 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
     const PathQueue NQ = E.q[cur ^ 1];
     const ShadowQueue SQ = E.sq;
     const float inv_pi = 1.f / 3.14159274f;
+    const int lane = threadIdx.x & 31;
     // warp-uniform trip count: every lane of a warp runs the same iterations,
     // so the warp-wide appends at the bottom see all 32 lanes
     const int stride = gridDim.x * blockDim.x;
@@ -274,48 +296,45 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
         float4 o4 = make_float4(0, 0, 0, 0), d4 = o4, tp4 = o4, h = o4;
         if (live) { id = Q.id[i]; o4 = Q.o[i]; d4 = Q.d[i]; tp4 = Q.tp[i]; h = E.hit[i]; }
         const int slot = id.x;
-        const DRequest& R = E.reqs[slot];
         const uint32_t prim = __float_as_uint(h.y);
         const int meta = __float_as_int(d4.w);
         const int bounce = meta & 0xFF, fork = (meta >> 8) & 7, single = (meta >> 11) & 1, nHero = (meta >> 12) & 7;
-        const bool spectral = live && (R.flags & kReqSpectral);
-        bool cont = false;            // continue into the next queue
-        int nfork = 0;                // forked sub-paths to emit
+        bool cont = false;    // continue into the next queue
+        int forked = 0;       // sub-paths written by a dispersive fork
         float3 no = make_float3(0, 0, 0), nd = no;
-        float ntp[4] = {0, 0, 0, 0};
-        float fork_o[4][3], fork_d[4][3], fork_tp[4], fork_lam[4];
+        float4 ntp = make_float4(0, 0, 0, 0);
         double* acc = nullptr;
         float3 emit_xyz = make_float3(0, 0, 0);
         bool emit = false;
 
-        // wavelengths carried by this path
-        float lam[4];
-        int nch = 1;
-        float wN = 1.f;
-        if (spectral) {
-            if (single) {
-                lam[0] = lam[1] = lam[2] = lam[3] = o4.w;
-                nch = 1;
-                wN = 1.f / (float)nHero;
-            } else {
-                const float span = 300.f, stride_l = span / (float)nHero;
-                lam[0] = o4.w;
-                for (int k = 1; k < 4; k++) {
-                    float l = lam[0] + stride_l * k;
-                    if (l > 700.f) l -= span;
-                    lam[k] = k < nHero ? l : lam[0];
-                }
-                nch = nHero;
-                wN = 1.f / (float)nHero;
-            }
-        } else {
-            lam[0] = lam[1] = lam[2] = lam[3] = 0.f;
-            nch = 3;
-        }
-        float tp[4] = {tp4.x, tp4.y, tp4.z, tp4.w};
-
         if (live && (prim & kPrimKindMask) != kPrimNone) {
+            const DRequest& R = E.reqs[slot];
             const DScene& S = E.scenes[R.scene];
+            const bool spectral = (R.flags & kReqSpectral) != 0;
+            // wavelengths carried by this path (code/Renderer.cpp:227-239)
+            float lam[4];
+            int nch = 3;
+            float wN = 1.f;
+            if (spectral) {
+                wN = 1.f / (float)nHero;
+                if (single) {
+                    lam[0] = lam[1] = lam[2] = lam[3] = o4.w;
+                    nch = 1;
+                } else {
+                    const float span = 300.f, stride_l = span / (float)nHero;
+                    lam[0] = o4.w;
+#pragma unroll
+                    for (int k = 1; k < 4; k++) {
+                        float l = lam[0] + stride_l * k;
+                        if (l > 700.f) l -= span;
+                        lam[k] = k < nHero ? l : lam[0];
+                    }
+                    nch = nHero;
+                }
+            } else {
+                lam[0] = lam[1] = lam[2] = lam[3] = 0.f;
+            }
+            const float tp[4] = {tp4.x, tp4.y, tp4.z, tp4.w};
             acc = R.accum + (size_t)id.y * 3;
             const float3 o = xyz(o4), d = xyz(d4);
             const float t = h.x;
@@ -326,8 +345,7 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
             if (kind == kPrimSphere) {
                 const float4 cr = S.spheres[pidx].c_r;
                 float3 v = make_float3(hit.x - cr.x, hit.y - cr.y, hit.z - cr.z);
-                float il = rsqrtf(f3dot(v, v));
-                N = f3mul(v, il);
+                N = f3mul(v, rsqrtf(f3dot(v, v)));
                 mi = S.spheres[pidx].mat.x;
             } else if (kind == kPrimPlane) {
                 const float4 na = S.planes[pidx].n_area;
@@ -352,8 +370,11 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
             const bool last = bounce + 1 >= R.depth;
             if (m.flags & kMatEmissive) {
                 float c[4] = {0.f, 0.f, 0.f, 0.f};
-                if (spectral) for (int k = 0; k < nch; k++) c[k] = tp[k] * emissive_at(m, lam[k]);
-                else { c[0] = tp[0] * m.emissive.x; c[1] = tp[1] * m.emissive.y; c[2] = tp[2] * m.emissive.z; }
+                if (spectral) {
+                    for (int k = 0; k < nch; k++) c[k] = tp[k] * emissive_at(m, lam[k]);
+                } else {
+                    c[0] = tp[0] * m.emissive.x; c[1] = tp[1] * m.emissive.y; c[2] = tp[2] * m.emissive.z;
+                }
                 const XyzWeights W = xyz_weights(spectral, lam, nch, wN, K.xyz_scale);
                 emit_xyz = apply_xyz(W, c);
                 emit = true;
@@ -362,8 +383,11 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
                     const float cosI = -f3dot(d, N);
                     nd = f3add(d, f3mul(N, 2.f * cosI));
                     no = f3add(hit, f3mul(N, 1e-3f));
-                    if (spectral) for (int k = 0; k < 4; k++) ntp[k] = tp[k] * albedo_at(m, lam[k]);
-                    else { ntp[0] = tp[0] * m.albedo.x; ntp[1] = tp[1] * m.albedo.y; ntp[2] = tp[2] * m.albedo.z; }
+                    if (spectral)
+                        ntp = make_float4(tp[0] * albedo_at(m, lam[0]), tp[1] * albedo_at(m, lam[1]),
+                                          tp[2] * albedo_at(m, lam[2]), tp[3] * albedo_at(m, lam[3]));
+                    else
+                        ntp = make_float4(tp[0] * m.albedo.x, tp[1] * m.albedo.y, tp[2] * m.albedo.z, 0.f);
                     cont = true;
                 }
             } else if (m.flags & kMatTransparent) {
@@ -372,10 +396,16 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
                     const bool disperse = spectral && m.cauchyB != 0.f && !single && nHero > 1;
                     const int ways = disperse ? nHero : 1;
                     const float4 coins = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 63u);
+                    int fpos = 0;
+                    if (disperse) {
+                        fpos = group_append(&C->queue_n[cur ^ 1], ways);
+                        forked = ways;
+                    }
                     for (int k = 0; k < ways; k++) {
                         float ior = m.ior;
                         if (spectral && m.cauchyB != 0.f && (disperse || single))
-                            ior = m.ior + m.cauchyB * 1e4f / (lam[k] * lam[k]);
+                            ior = m.ior + m.cauchyB * 1e4f / (lam[k] * lam[k]);  // Optics::cauchyIor
+                        // Optics::dielectricBounce (code/Includes/Optics.h:59-82)
                         const float n1 = entering ? 1.f : ior, n2 = entering ? ior : 1.f;
                         const float eta = n1 / n2;
                         const float sinT2 = eta * eta * (1.f - cosI * cosI);
@@ -397,35 +427,53 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
                             bo = f3sub(hit, f3mul(N, 1e-3f));
                         }
                         if (disperse) {
-                            fork_o[k][0] = bo.x; fork_o[k][1] = bo.y; fork_o[k][2] = bo.z;
-                            fork_d[k][0] = bd.x; fork_d[k][1] = bd.y; fork_d[k][2] = bd.z;
-                            fork_tp[k] = tp[k] * albedo_at(m, lam[k]);
-                            fork_lam[k] = lam[k];
+                            // sub-path k carries wavelength k alone (code/Renderer.cpp:736-753)
+                            const int pos = fpos + k;
+                            if (pos < E.queue_cap) {
+                                const float ftp = tp[k] * albedo_at(m, lam[k]);
+                                const int fm = (bounce + 1) | ((k + 1) << 8) | (1 << 11) | (nHero << 12);
+                                NQ.o[pos] = make_float4(bo.x, bo.y, bo.z, lam[k]);
+                                NQ.d[pos] = make_float4(bd.x, bd.y, bd.z, __int_as_float(fm));
+                                NQ.tp[pos] = make_float4(ftp, ftp, ftp, ftp);
+                                NQ.id[pos] = id;
+                            } else {
+                                atomicOr(&C->status, 2);
+                            }
                         } else {
                             no = bo;
                             nd = bd;
                         }
                     }
-                    if (disperse) {
-                        nfork = ways;
-                    } else {
-                        if (spectral) for (int k = 0; k < 4; k++) ntp[k] = tp[k] * albedo_at(m, lam[k]);
-                        else { ntp[0] = tp[0] * m.albedo.x; ntp[1] = tp[1] * m.albedo.y; ntp[2] = tp[2] * m.albedo.z; }
+                    if (!disperse) {
+                        if (spectral)
+                            ntp = make_float4(tp[0] * albedo_at(m, lam[0]), tp[1] * albedo_at(m, lam[1]),
+                                              tp[2] * albedo_at(m, lam[2]), tp[3] * albedo_at(m, lam[3]));
+                        else
+                            ntp = make_float4(tp[0] * m.albedo.x, tp[1] * m.albedo.y, tp[2] * m.albedo.z, 0.f);
                         cont = true;
                     }
                 }
             } else {
                 // diffuse
-                float al[4];
-                if (spectral) for (int k = 0; k < nch; k++) al[k] = albedo_at(m, lam[k]);
-                else { al[0] = m.albedo.x; al[1] = m.albedo.y; al[2] = m.albedo.z; }
+                float al[4] = {0.f, 0.f, 0.f, 0.f};
+                if (spectral) {
+                    for (int k = 0; k < nch; k++) al[k] = albedo_at(m, lam[k]);
+                } else {
+                    al[0] = m.albedo.x; al[1] = m.albedo.y; al[2] = m.albedo.z;
+                }
                 // indirect origin: hit moved once by 1e-3*N (the reference's
                 // mutating `hit + N * 1e-3`, code/Renderer.cpp:782 with samples = 1)
                 float3 hc = f3add(hit, f3mul(N, 1e-3f));
                 const float3 h1 = hc;
                 if (S.total_light_area > 0.f) {
-                    const float invS = 1.f / (float)R.shadow;
+                    const float scaleS = S.total_light_area * inv_pi / (float)R.shadow;
                     const XyzWeights W = xyz_weights(spectral, lam, nch, wN, K.xyz_scale);
+                    float tpal[4];
+#pragma unroll
+                    for (int k = 0; k < 4; k++) tpal[k] = tp[k] * al[k];
+                    int cached = -1;
+                    float3 V = make_float3(0.f, 0.f, 0.f);
+                    int spos = group_append(&C->shadow_n, R.shadow);
                     for (int s = 0; s < R.shadow; s++) {
                         const float4 rr = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce,
                                                 1u + (uint32_t)s);
@@ -474,44 +522,34 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
                         else { hc = f3add(hc, f3mul(N, 1e-3f)); so = hc; }
                         const float cosL = fmaxf(0.f, -f3dot(Nl, Li));
                         const float G = (cosT * cosL) / d2;
-                        const bool useful = G > 0.f;
-                        float3 cx = make_float3(0.f, 0.f, 0.f);
-                        if (useful) {
-                            float w = 1.f;
-                            if ((R.flags & kReqMIS) && cosL > 1e-6f) {
-                                const float pL = d2 / (cosL * S.total_light_area), pB = cosT * inv_pi;
-                                w = (pL * pL) / (pL * pL + pB * pB);
-                            }
+                        const int pos = spos + s;
+                        if (pos >= E.shadow_cap) { atomicOr(&C->status, 1); continue; }
+                        if (!(G > 0.f)) {
+                            SQ.o[pos] = make_float4(0.f, 0.f, 0.f, -1.f);  // skip record
+                            continue;
+                        }
+                        if (lm != cached) {
+                            // spectral product of this light material, once per vertex
                             const DMaterial& lmat = M[S.mat_base + lm];
-                            const float f = G * S.total_light_area * w * invS * inv_pi;
                             float c[4] = {0.f, 0.f, 0.f, 0.f};
-                            if (spectral) for (int k = 0; k < nch; k++) c[k] = tp[k] * al[k] * emissive_at(lmat, lam[k]) * f;
-                            else {
-                                c[0] = tp[0] * al[0] * lmat.emissive.x * f;
-                                c[1] = tp[1] * al[1] * lmat.emissive.y * f;
-                                c[2] = tp[2] * al[2] * lmat.emissive.z * f;
-                            }
-                            cx = apply_xyz(W, c);
-                        }
-                        // append among the lanes that reach this point
-                        namespace cg = cooperative_groups;
-                        cg::coalesced_group g = cg::coalesced_threads();
-                        const int want = useful ? 1 : 0;
-                        const int ex = cg::exclusive_scan(g, want);
-                        const int tot = g.shfl(ex + want, g.size() - 1);
-                        int sbase = 0;
-                        if (g.thread_rank() == 0 && tot) sbase = atomicAdd(&C->shadow_n, tot);
-                        sbase = g.shfl(sbase, 0);
-                        if (useful) {
-                            const int pos = sbase + ex;
-                            if (pos < E.shadow_cap) {
-                                SQ.o[pos] = make_float4(so.x, so.y, so.z, d2);
-                                SQ.d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(id.y));
-                                SQ.c[pos] = make_float4(cx.x, cx.y, cx.z, __int_as_float(slot));
+                            if (spectral) {
+                                for (int k = 0; k < nch; k++) c[k] = tpal[k] * emissive_at(lmat, lam[k]);
                             } else {
-                                atomicOr(&C->status, 1);
+                                c[0] = tpal[0] * lmat.emissive.x; c[1] = tpal[1] * lmat.emissive.y;
+                                c[2] = tpal[2] * lmat.emissive.z;
                             }
+                            V = f3mul(apply_xyz(W, c), scaleS);
+                            cached = lm;
                         }
+                        float w = 1.f;
+                        if ((R.flags & kReqMIS) && cosL > 1e-6f) {
+                            const float pL = d2 / (cosL * S.total_light_area), pB = cosT * inv_pi;
+                            w = (pL * pL) / (pL * pL + pB * pB);
+                        }
+                        const float f = G * w;
+                        SQ.o[pos] = make_float4(so.x, so.y, so.z, d2);
+                        SQ.d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(id.y));
+                        SQ.c[pos] = make_float4(V.x * f, V.y * f, V.z * f, __int_as_float(slot));
                     }
                 }
                 const float4 r0 = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 0u);
@@ -533,7 +571,8 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
                     }
                     nd = hemisphere(N, r1, r2);
                     no = h1;
-                    for (int k = 0; k < 4; k++) ntp[k] = tp[k] * (k < (spectral ? nch : 3) ? al[k] : 0.f) * rr_scale;
+                    ntp = make_float4(tp[0] * al[0] * rr_scale, tp[1] * al[1] * rr_scale, tp[2] * al[2] * rr_scale,
+                                      tp[3] * al[3] * rr_scale);
                     cont = true;
                 }
             }
@@ -541,34 +580,24 @@ __global__ void k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
 
         // ---- emit work (warp-uniform control flow from here)
         if (emit) add_xyz(acc, emit_xyz);
-        const int newMeta = (bounce + 1) | (fork << 8) | (single << 11) | (nHero << 12);
         {
+            const int newMeta = (bounce + 1) | (fork << 8) | (single << 11) | (nHero << 12);
             int pos = warp_append(&C->queue_n[cur ^ 1], cont);
             if (pos >= E.queue_cap) { atomicOr(&C->status, 2); pos = -1; }
             if (pos >= 0) {
                 NQ.o[pos] = make_float4(no.x, no.y, no.z, o4.w);
                 NQ.d[pos] = make_float4(nd.x, nd.y, nd.z, __int_as_float(newMeta));
-                NQ.tp[pos] = make_float4(ntp[0], ntp[1], ntp[2], ntp[3]);
+                NQ.tp[pos] = ntp;
                 NQ.id[pos] = id;
             }
         }
-        for (int k = 0; k < 4; k++) {
-            int pos = warp_append(&C->queue_n[cur ^ 1], k < nfork);
-            if (pos >= E.queue_cap) { atomicOr(&C->status, 2); pos = -1; }
-            if (pos >= 0) {
-                const int fm = (bounce + 1) | ((k + 1) << 8) | (1 << 11) | (nHero << 12);
-                NQ.o[pos] = make_float4(fork_o[k][0], fork_o[k][1], fork_o[k][2], fork_lam[k]);
-                NQ.d[pos] = make_float4(fork_d[k][0], fork_d[k][1], fork_d[k][2], __int_as_float(fm));
-                NQ.tp[pos] = make_float4(fork_tp[k], fork_tp[k], fork_tp[k], fork_tp[k]);
-                NQ.id[pos] = id;
-            }
-            if (!__any_sync(0xffffffffu, k + 1 < nfork)) break;
-        }
-        // path bookkeeping: -1 for a retired path, +ways-1 for a fork
-        if (live) {
-            const long long delta = (cont ? 0 : -1) + (nfork > 0 ? nfork : 0);
-            if (delta != 0) atomicAdd((unsigned long long*)&E.outstanding[slot], (unsigned long long)delta);
-        }
+        // path bookkeeping per request, one atomic per request per warp:
+        // -1 for a retired path, ways-1 for a fork
+        const long long delta = live ? (long long)((cont ? 0 : -1) + forked) : 0;
+        const unsigned same = __match_any_sync(0xffffffffu, live ? slot : -1);
+        const int sum = __reduce_add_sync(same, (int)delta);
+        if (live && sum != 0 && lane == __ffs(same) - 1)
+            atomicAdd((unsigned long long*)&E.outstanding[slot], (unsigned long long)(long long)sum);
     }
 }
 
@@ -584,7 +613,9 @@ __global__ void k_shadow(EngineView E)
     const ShadowQueue SQ = E.sq;
     unsigned long long mine = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4 o = SQ.o[i], d = SQ.d[i], c = SQ.c[i];
+        const float4 o = SQ.o[i];
+        if (!(o.w >= 0.f)) continue;  // skip record (zero geometry term)
+        const float4 d = SQ.d[i], c = SQ.c[i];
         const int slot = __float_as_int(c.w);
         const DRequest& R = E.reqs[slot];
         const DScene& S = E.scenes[R.scene];

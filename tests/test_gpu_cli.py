@@ -1,0 +1,48 @@
+"""The reference-facing surface on the GPU: the `pcr-render` CLI (same flags
+as code/Cli/Main.cpp) writes a PNG whose name pattern and tEXt keys match the
+reference renderer's (code/Renderer.cpp:393-447) and whose pixels are the
+library's tone-mapped output for the same request."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, REPO, scene_path
+
+pytestmark = pytest.mark.gpu
+
+CLI = os.path.join(REPO, "pcr_b200", "lib", "pcr-render")
+
+
+def test_cli_png_matches_library_and_reference_format(tmp_path):
+    from PIL import Image
+
+    from pcr_b200 import build, capi
+    build.build()
+    args = [CLI, "--scenes-dir", os.path.join(GOLDEN, "scenes"), "--scene", "cornell", "-w", "64", "--height", "48",
+            "-d", "3", "-s", "8", "-S", "2", "--spectral", "--seed", "77", "-o", str(tmp_path)]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    assert "Render took" in out.stdout and "Wrote" in out.stdout
+    files = os.listdir(tmp_path)
+    assert len(files) == 1
+    name = files[0]
+    assert re.match(r"cornell-1\.1\.0-\d{8}-\d{6}-[A-Z]+-d3-s8-S2-w64-h48-spectral-t\d+\.png$", name), name
+    img = Image.open(tmp_path / name)
+    golden = Image.open(os.path.join(GOLDEN, "render", "cornell-spectral.png"))
+    assert list(img.text.keys()) == list(golden.text.keys())
+    assert img.text["Spectral"] == "1" and img.text["Depth"] == "3" and img.text["Tonemap"] == "Reinhard"
+    rgb = np.asarray(img.convert("RGB"))
+    ctx = capi.Context()
+    sid = ctx.load_scene_json(scene_path("cornell"), GOLDEN)
+    _, lib_rgb, _ = ctx.render(sid, capi.render_desc(64, 48, depth=3, samples=8, shadow=2, spectral=True, seed=77))
+    ctx.close()
+    assert np.array_equal(rgb, lib_rgb)
+
+
+def test_cli_rejects_unknown_scene():
+    out = subprocess.run([CLI, "--scenes-dir", os.path.join(GOLDEN, "scenes"), "--scene", "nope"],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode == 1 and "Unknown scene" in out.stderr
