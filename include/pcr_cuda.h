@@ -160,6 +160,28 @@ pcr_status pcr_scene_bytes(pcr_ctx *ctx, pcr_scene_id id, int64_t *bytes);
 pcr_status pcr_render(pcr_ctx *ctx, pcr_scene_id scene, const pcr_render_desc *desc,
                       float *hdr_out, uint8_t *rgb8_out, pcr_render_stats *stats);
 
+/* Plain render that allocates nothing.  This entry point has no counterpart
+ * in the reference; it exists for callers that may not allocate device
+ * memory while they render: a host that has handed all device memory to its
+ * own pool allocator, or a real-time loop that cannot afford cudaMalloc /
+ * cudaFree, which synchronize the whole device and stall every other stream.
+ * All working memory (path and shadow queues, hit records, the FP64 pixel
+ * accumulator, request and counter words) comes from one fixed array of
+ * about 18 MiB compiled into the library, which every GPU that loads the
+ * library holds until the process exits.
+ *   - scene: a scene already uploaded to ctx (an input; not copied again).
+ *   - hdr_out_dev / rgb8_out_dev: caller-owned DEVICE buffers of W*H*3 floats /
+ *     bytes (either may be NULL, not both), written as pcr_render writes them.
+ *   - Limits: at most 65536 pixels (e.g. 256x256) and at most 8 shadow samples
+ *     per hit; larger requests return PCR_ERR_INVALID.
+ * The first call on a device looks up the array's device address on that
+ * device (cudaGetSymbolAddress); make that first call before any stream
+ * capture.  Every call shares the one array and clears what must start at
+ * zero, so calls that overlap on the GPU (from several threads, or several
+ * contexts on one device) race; serialise them.  Synchronous. */
+pcr_status pcr_render_noalloc(pcr_ctx *ctx, pcr_scene_id scene, const pcr_render_desc *desc,
+                              float *hdr_out_dev, uint8_t *rgb8_out_dev);
+
 /* Batched / served method.  pcr_submit is thread-safe and returns at once;
  * the request is admitted into the shared wavefront when the memory budget
  * and queue allow.  pcr_run_until_idle drives the engine on the calling

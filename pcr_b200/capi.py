@@ -23,7 +23,7 @@ STATUS = {0: "PCR_OK", 1: "PCR_ERR_INVALID", 2: "PCR_ERR_CUDA", 3: "PCR_ERR_NO_M
 EXPORTS = [
     "pcr_last_error", "pcr_version", "pcr_ctx_create", "pcr_ctx_destroy", "pcr_ctx_set_device", "pcr_ctx_stream",
     "pcr_scene_upload", "pcr_scene_load_json", "pcr_host_scene_load", "pcr_host_scene_free",
-    "pcr_fit_sigmoid", "pcr_lut_build", "pcr_scene_release", "pcr_scene_bytes", "pcr_render",
+    "pcr_fit_sigmoid", "pcr_lut_build", "pcr_scene_release", "pcr_scene_bytes", "pcr_render", "pcr_render_noalloc",
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
     "pcr_fetch", "pcr_cancel", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
     "pcr_trace_closest", "pcr_trace_bvh", "pcr_eval_stage",
@@ -138,6 +138,7 @@ def load_library():
         "pcr_lut_build": [fp],
         "pcr_scene_bytes": [P, C.c_int32, C.POINTER(C.c_int64)],
         "pcr_render": [P, C.c_int32, C.POINTER(RenderDesc), fp, up, C.POINTER(RenderStats)],
+        "pcr_render_noalloc": [P, C.c_int32, C.POINTER(RenderDesc), fp, up],
         "pcr_submit": [P, C.c_int32, C.POINTER(RenderDesc), C.POINTER(C.c_int64)],
         "pcr_run_until_idle": [P],
         "pcr_serve_start": [P],
@@ -314,6 +315,13 @@ class Context:
         _check(self.L.pcr_render(self.h, sid, C.byref(desc), _fp(hdr) if want_hdr else None,
                                  rgb.ctypes.data_as(C.POINTER(C.c_uint8)) if want_rgb else None, C.byref(st)))
         return hdr, rgb, st
+
+    def render_noalloc(self, sid: int, desc: RenderDesc, hdr_dev_ptr: int, rgb_dev_ptr: int) -> None:
+        """Plain render that allocates no device memory (pcr_render_noalloc):
+        outputs go to caller-owned device buffers given as raw pointers."""
+        _check(self.L.pcr_render_noalloc(self.h, sid, C.byref(desc), C.cast(C.c_void_p(hdr_dev_ptr), C.POINTER(C.c_float))
+                                         if hdr_dev_ptr else None,
+                                         C.cast(C.c_void_p(rgb_dev_ptr), C.POINTER(C.c_uint8)) if rgb_dev_ptr else None))
 
     def submit(self, sid: int, desc: RenderDesc) -> int:
         rid = C.c_int64()

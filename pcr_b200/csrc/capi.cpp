@@ -179,6 +179,15 @@ pcr_status pcr_render(pcr_ctx* ctx, pcr_scene_id scene, const pcr_render_desc* d
     });
 }
 
+pcr_status pcr_render_noalloc(pcr_ctx* ctx, pcr_scene_id scene, const pcr_render_desc* desc, float* hdr_out_dev,
+                              uint8_t* rgb8_out_dev)
+{
+    return guard([&] {
+        if (!desc) throw pcr::PcrError(PCR_ERR_INVALID, "null render descriptor");
+        E(ctx).render_noalloc(scene, *desc, hdr_out_dev, rgb8_out_dev);
+    });
+}
+
 pcr_status pcr_submit(pcr_ctx* ctx, pcr_scene_id scene, const pcr_render_desc* desc, pcr_request_id* out)
 {
     return guard([&] {

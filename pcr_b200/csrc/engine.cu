@@ -983,6 +983,223 @@ void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, ui
     }
 }
 
+// ---------------------------------------------------------------- render without allocating
+// pcr_render_noalloc: a plain render whose working memory (path queues, hit
+// records, shadow queue, FP64 pixel accumulator, request and counter words)
+// is carved from one fixed-size array compiled into this library, for
+// callers that may not allocate device memory during a render.  Inputs are
+// a scene already uploaded to the context; outputs are caller-owned device
+// buffers.  Every GPU that loads the library holds the array until exit.
+constexpr int kNoAllocFill = 8192;                       // paths per pass
+constexpr int kNoAllocQueue = kNoAllocFill * 4;          // room for 4-way forks
+constexpr int kNoAllocShadowPerVertex = 8;
+constexpr int kNoAllocShadow = kNoAllocQueue * kNoAllocShadowPerVertex;
+constexpr int64_t kNoAllocMaxPixels = 256 * 256;
+constexpr size_t kNoAllocAlign = 256;
+constexpr size_t align_up(size_t x) { return (x + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
+constexpr size_t kNoAllocHeader = 64 * 1024;             // counters, request table, per-slot words
+constexpr size_t kNoAllocQueueBytes = align_up((size_t)kNoAllocQueue * 64);
+constexpr size_t kNoAllocHitBytes = align_up((size_t)kNoAllocQueue * 16);
+constexpr size_t kNoAllocShadowBytes = align_up((size_t)kNoAllocShadow * 48);
+constexpr size_t kNoAllocAccumBytes = align_up((size_t)kNoAllocMaxPixels * 3 * sizeof(double));
+constexpr size_t kNoAllocBytes =
+    kNoAllocHeader + 2 * kNoAllocQueueBytes + kNoAllocHitBytes + kNoAllocShadowBytes + kNoAllocAccumBytes;
+
+// The scratch array.  In host code `g_noalloc_scratch` is only a host-side
+// stand-in for the symbol; its device address comes from
+// cudaGetSymbolAddress (noalloc_scratch() below), once per device.
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[128] = {nullptr};
+}  // namespace
+
+// Device address of the scratch array on `device` (which must be current).
+// Looked up on the first call per device; later calls reuse it.
+static void* noalloc_scratch(int device)
+{
+    if (device < 0 || device >= 128) throw PcrError(PCR_ERR_INVALID, "device ordinal out of range");
+    std::lock_guard<std::mutex> g(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p)
+            throw PcrError(PCR_ERR_CUDA, std::string("cudaGetSymbolAddress(scratch): ") + cudaGetErrorString(e));
+        g_noalloc_ptr[device] = p;
+    }
+    return g_noalloc_ptr[device];
+}
+
+// The request entry of a render (same fields Engine::activate writes).
+DRequest Engine::make_request(const pcr_render_desc& d, int scene, double* accum) const
+{
+    const SceneEntry& S = scenes_[scene];
+    DRequest R{};
+    R.scene = scene;
+    R.width = d.width;
+    R.height = d.height;
+    R.depth = d.depth;
+    R.aa = std::max(1, d.aa_samples);
+    R.spp = d.samples;
+    R.paths_per_pixel = R.aa * R.spp;
+    R.shadow = d.shadow_samples;
+    R.flags = (d.spectral ? kReqSpectral : 0) | (d.mis ? kReqMIS : 0) | (d.russian ? kReqRussian : 0) |
+              (d.stratified ? kReqStratified : 0);
+    R.hero = std::min(4, std::max(1, d.hero_samples <= 0 ? 4 : d.hero_samples));
+    R.strata = d.stratified ? std::max(1, (int)std::lround(std::sqrt((float)d.samples))) : 0;
+    R.cam_x = S.cam[0];
+    R.cam_y = S.cam[1];
+    R.cam_z = S.cam[2];
+    R.aspect = d.width / (float)d.height;
+    R.scale = std::tan((float)3.14159265358979323846 / 180.f * 0.5f * S.fov);
+    const uint64_t seed = d.seed ? d.seed : 1ull;
+    R.seed_lo = (uint32_t)(seed & 0xffffffffu) * 0x9E3779B1u + 0x7F4A7C15u;
+    R.seed_hi = (uint32_t)(seed >> 32) ^ (uint32_t)(seed * 0xD1B54A32D192ED03ull >> 17);
+    R.total = (int64_t)d.width * d.height * R.paths_per_pixel;
+    R.accum = accum;
+    return R;
+}
+
+void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_dev, uint8_t* rgb_dev)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    validate(scene, desc);
+    const int64_t px = (int64_t)desc.width * desc.height;
+    if (px > kNoAllocMaxPixels)
+        throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: " + std::to_string(desc.width) + "x" +
+                                            std::to_string(desc.height) + " exceeds the " +
+                                            std::to_string(kNoAllocMaxPixels) + "-pixel limit of its fixed scratch");
+    if (desc.shadow_samples > kNoAllocShadowPerVertex)
+        throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: more than " + std::to_string(kNoAllocShadowPerVertex) +
+                                            " shadow samples per hit");
+    if (!hdr_dev && !rgb_dev) throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: no output buffer");
+    if (!active_slots_.empty() || serving_)
+        throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc while batched work is active");
+
+    unsigned char* base = static_cast<unsigned char*>(noalloc_scratch(device_));
+    // carve the array: header words first, then queues, hits, shadows, accumulator
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        unsigned char* p = base + off;
+        off += align_up(bytes);
+        return p;
+    };
+    Counters* cnt = reinterpret_cast<Counters*>(take(sizeof(Counters)));
+    EngineParams* params = reinterpret_cast<EngineParams*>(take(sizeof(EngineParams)));
+    DRequest* reqs = reinterpret_cast<DRequest*>(take(sizeof(DRequest)));
+    unsigned long long* issued = reinterpret_cast<unsigned long long*>(take(8));
+    long long* outstanding = reinterpret_cast<long long*>(take(8));
+    unsigned long long* tfirst = reinterpret_cast<unsigned long long*>(take(8));
+    unsigned long long* tdone = reinterpret_cast<unsigned long long*>(take(8));
+    long long* give_start = reinterpret_cast<long long*>(take(8));
+    int* give = reinterpret_cast<int*>(take(4));
+    int* give_base = reinterpret_cast<int*>(take(4));
+    int* active = reinterpret_cast<int*>(take(4));
+    int* n_active = reinterpret_cast<int*>(take(4));
+    int* done = reinterpret_cast<int*>(take(4));
+    const size_t header_used = off;
+    off = kNoAllocHeader;
+    PathQueue q[2];
+    for (int b = 0; b < 2; b++) {
+        unsigned char* p = take(kNoAllocQueueBytes);
+        q[b].o = reinterpret_cast<float4*>(p);
+        q[b].d = q[b].o + kNoAllocQueue;
+        q[b].tp = q[b].d + kNoAllocQueue;
+        q[b].id = reinterpret_cast<int4*>(q[b].tp + kNoAllocQueue);
+    }
+    float4* hit = reinterpret_cast<float4*>(take(kNoAllocHitBytes));
+    ShadowQueue sq;
+    sq.o = reinterpret_cast<float4*>(take(kNoAllocShadowBytes));
+    sq.d = sq.o + kNoAllocShadow;
+    sq.c = sq.d + kNoAllocShadow;
+    double* accum = reinterpret_cast<double*>(take(kNoAllocAccumBytes));
+    if (off > kNoAllocBytes || header_used > kNoAllocHeader)
+        throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: scratch layout overflow");
+
+    // the array keeps the previous call's contents: clear what starts at zero
+    CK(cudaMemsetAsync(base, 0, header_used, stream_));
+    CK(cudaMemsetAsync(accum, 0, (size_t)px * 3 * sizeof(double), stream_));
+
+    EngineView E{};
+    E.scenes = d_scenes_;
+    E.mats = d_mats_;
+    E.reqs = reqs;
+    E.issued = issued;
+    E.outstanding = outstanding;
+    E.give = give;
+    E.give_base = give_base;
+    E.active = active;
+    E.n_active = n_active;
+    E.done_flag = done;
+    E.t_first = tfirst;
+    E.t_done = tdone;
+    E.cnt = cnt;
+    E.q[0] = q[0];
+    E.q[1] = q[1];
+    E.hit = hit;
+    E.sq = sq;
+    E.give_start = give_start;
+    E.shadow_cap = kNoAllocShadow;
+    E.queue_cap = kNoAllocQueue;
+    E.n_mats = mat_count_;
+
+    DRequest R = make_request(desc, scene, accum);
+    k_admit<<<1, 1, 0, stream_>>>(E, R, 0);
+    ActiveList L;
+    L.n = 1;
+    L.slots[0] = 0;
+    k_set_active<<<1, 32, 0, stream_>>>(E, L);
+    const int pass = (int)std::min<int64_t>(px, kNoAllocFill);
+    k_set_params<<<1, 1, 0, stream_>>>(params, EngineParams{pass, pass, 1, 1});
+    CK(cudaGetLastError());
+
+    // launch shapes from the occupancy calculator (no allocation involved)
+    const int B = tune_.block_size;
+    const size_t mat_bytes = sizeof(DMaterial) * (size_t)std::max(1, mat_count_);
+    const int smem_mats = mat_bytes <= 96 * 1024 ? 1 : 0;
+    const size_t smem = smem_mats ? mat_bytes : 0;
+    CK(cudaFuncSetAttribute(k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int g_regen, g_extend, g_shade, g_shadow;
+    grid_for((const void*)k_regen, B, 0, &g_regen);
+    grid_for((const void*)k_extend, B, 0, &g_extend);
+    grid_for((const void*)k_shade, B, smem, &g_shade);
+    grid_for((const void*)k_shadow, B, 0, &g_shadow);
+    ShadeConst K{xyz_scale_};
+    int cur = 0;
+    auto iteration = [&]() {
+        k_schedule<<<1, kSchedThreads, 0, stream_>>>(E, params, cur);
+        k_regen<<<g_regen, B, 0, stream_>>>(E, cur);
+        k_extend<<<g_extend, B, 0, stream_>>>(E, cur);
+        k_shade<<<g_shade, B, smem, stream_>>>(E, cur, K, smem_mats);
+        k_shadow<<<g_shadow, B, 0, stream_>>>(E);
+        k_status<<<1, 1024, 0, stream_>>>(E, cur ^ 1);
+        CK(cudaGetLastError());
+        cur ^= 1;
+    };
+    const int64_t total = px * desc.samples * std::max(1, desc.aa_samples);
+    const int64_t passes = (total + pass - 1) / pass;
+    for (int64_t it = 0; it < passes * (int64_t)desc.depth; it++) iteration();
+    for (int extra = 0;; extra++) {
+        int flag = 0;
+        Counters c;
+        CK(cudaMemcpyAsync(&flag, done, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(&c, cnt, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        if (c.status) throw PcrError(PCR_ERR_DEVICE_STATUS, "pcr_render_noalloc: device reported queue overflow");
+        if (flag) break;
+        if (extra > 4 * desc.depth + 8) throw PcrError(PCR_ERR_TIMEOUT, "pcr_render_noalloc did not finish");
+        iteration();
+    }
+    const double inv = 1.0 / ((double)desc.samples * std::max(1, desc.aa_samples));
+    const int grid = (int)std::min<int64_t>((px + 255) / 256, (int64_t)sms_ * 8);
+    k_resolve<<<std::max(1, grid), 256, 0, stream_>>>(accum, (int)px, inv, desc.spectral ? 1 : 0, desc.aces ? 1 : 0,
+                                                       hdr_dev, rgb_dev);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
+}
+
 // ---------------------------------------------------------------- parity entry points
 void Engine::trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_t* prim, float* t, int bvh_only,
                    int32_t* counts)

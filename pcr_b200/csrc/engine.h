@@ -72,6 +72,9 @@ public:
     int64_t scene_bytes(int id) const;
 
     void render_plain(int scene, const pcr_render_desc& desc, float* hdr, uint8_t* rgb, pcr_render_stats* st);
+    // Plain render with all working memory in the library's fixed scratch
+    // array; outputs are caller device buffers.  Allocates nothing.
+    void render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_dev, uint8_t* rgb_dev);
     int64_t submit(int scene, const pcr_render_desc& desc);
     void run_until_idle();
     void serve_start();
@@ -107,6 +110,7 @@ private:
     void harvest(bool final_sync);
     void finish_request(Request& r);
     void copy_out(Request& r, float* hdr, uint8_t* rgb);
+    DRequest make_request(const pcr_render_desc& d, int scene, double* accum) const;
     void check_status();
     bool engine_step();
     void serve_loop();
