@@ -327,9 +327,10 @@ def main():
         # algorithmic bytes per unit (queue records, 16-byte words):
         #   extend: ray in (origin, dir, id: 48 B) + hit out (16 B)
         #   shadow: shadow record in (48 B)
-        #   shade : path in (64 B) + hit in (16 B) + path out (64 B) + shadow out (48 B each)
+        #   shade : spectral path in (o, d, tp, id, XYZ weights: 112 B) + hit in (16 B)
+        #           + path out (112 B) + shadow out (48 B each)
         bytes_stage = {"extend": 64.0 * ps["rays"], "shadow": 48.0 * ps["shadow_rays"],
-                       "shade": 144.0 * ps["rays"] + 48.0 * ps["shadow_rays"]}
+                       "shade": 240.0 * ps["rays"] + 48.0 * ps["shadow_rays"]}
         dom = max(bytes_stage, key=lambda k: ps["stage_ms"][k])
         t_ms = ps["stage_ms"][dom]
         n_l = max(1, ps["stage_launches"][dom])

@@ -167,7 +167,7 @@ pcr_status pcr_render(pcr_ctx *ctx, pcr_scene_id scene, const pcr_render_desc *d
  * cudaFree, which synchronize the whole device and stall every other stream.
  * All working memory (path and shadow queues, hit records, the FP64 pixel
  * accumulator, request and counter words) comes from one fixed array of
- * about 18 MiB compiled into the library, which every GPU that loads the
+ * about 21 MiB compiled into the library, which every GPU that loads the
  * library holds until the process exits.
  *   - scene: a scene already uploaded to ctx (an input; not copied again).
  *   - hdr_out_dev / rgb8_out_dev: caller-owned DEVICE buffers of W*H*3 floats /

@@ -170,6 +170,7 @@ void Engine::alloc_buffers()
         q_[b].d = dalloc<float4>(queue_cap_, T);
         q_[b].tp = dalloc<float4>(queue_cap_, T);
         q_[b].id = dalloc<int4>(queue_cap_, T);
+        for (int k = 0; k < 3; k++) q_[b].w[k] = dalloc<float4>(queue_cap_, T);
     }
     d_hit_ = dalloc<float4>(queue_cap_, T);
     sq_.o = dalloc<float4>(shadow_cap_, T);
@@ -594,15 +595,14 @@ void Engine::launch_iteration(int cur, bool prof)
 {
     const EngineView E = view();
     const int B = tune_.block_size;
-    ShadeConst K{xyz_scale_};
     if (prof) CK(cudaEventRecord(prof_ev_[0], stream_));
     k_schedule<<<1, kSchedThreads, 0, stream_>>>(E, (const EngineParams*)d_params_, cur);
     if (prof) CK(cudaEventRecord(prof_ev_[1], stream_));
-    k_regen<<<grid_regen_, B, 0, stream_>>>(E, cur);
+    k_regen<<<grid_regen_, B, 0, stream_>>>(E, cur, xyz_scale_);
     if (prof) CK(cudaEventRecord(prof_ev_[2], stream_));
     k_extend<<<grid_extend_, B, 0, stream_>>>(E, cur);
     if (prof) CK(cudaEventRecord(prof_ev_[3], stream_));
-    k_shade<<<grid_shade_, B, shade_smem_, stream_>>>(E, cur, K, smem_mats_);
+    k_shade<<<grid_shade_, B, shade_smem_, stream_>>>(E, cur, smem_mats_);
     if (prof) CK(cudaEventRecord(prof_ev_[4], stream_));
     k_shadow<<<grid_shadow_, B, 0, stream_>>>(E);
     if (prof) CK(cudaEventRecord(prof_ev_[5], stream_));
@@ -998,7 +998,7 @@ constexpr int64_t kNoAllocMaxPixels = 256 * 256;
 constexpr size_t kNoAllocAlign = 256;
 constexpr size_t align_up(size_t x) { return (x + kNoAllocAlign - 1) / kNoAllocAlign * kNoAllocAlign; }
 constexpr size_t kNoAllocHeader = 64 * 1024;             // counters, request table, per-slot words
-constexpr size_t kNoAllocQueueBytes = align_up((size_t)kNoAllocQueue * 64);
+constexpr size_t kNoAllocQueueBytes = align_up((size_t)kNoAllocQueue * 112);  // 7 x 16 B per path
 constexpr size_t kNoAllocHitBytes = align_up((size_t)kNoAllocQueue * 16);
 constexpr size_t kNoAllocShadowBytes = align_up((size_t)kNoAllocShadow * 48);
 constexpr size_t kNoAllocAccumBytes = align_up((size_t)kNoAllocMaxPixels * 3 * sizeof(double));
@@ -1108,6 +1108,9 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
         q[b].d = q[b].o + kNoAllocQueue;
         q[b].tp = q[b].d + kNoAllocQueue;
         q[b].id = reinterpret_cast<int4*>(q[b].tp + kNoAllocQueue);
+        q[b].w[0] = reinterpret_cast<float4*>(q[b].id + kNoAllocQueue);
+        q[b].w[1] = q[b].w[0] + kNoAllocQueue;
+        q[b].w[2] = q[b].w[1] + kNoAllocQueue;
     }
     float4* hit = reinterpret_cast<float4*>(take(kNoAllocHitBytes));
     ShadowQueue sq;
@@ -1166,13 +1169,12 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     grid_for((const void*)k_extend, B, 0, &g_extend);
     grid_for((const void*)k_shade, B, smem, &g_shade);
     grid_for((const void*)k_shadow, B, 0, &g_shadow);
-    ShadeConst K{xyz_scale_};
     int cur = 0;
     auto iteration = [&]() {
         k_schedule<<<1, kSchedThreads, 0, stream_>>>(E, params, cur);
-        k_regen<<<g_regen, B, 0, stream_>>>(E, cur);
+        k_regen<<<g_regen, B, 0, stream_>>>(E, cur, xyz_scale_);
         k_extend<<<g_extend, B, 0, stream_>>>(E, cur);
-        k_shade<<<g_shade, B, smem, stream_>>>(E, cur, K, smem_mats);
+        k_shade<<<g_shade, B, smem, stream_>>>(E, cur, smem_mats);
         k_shadow<<<g_shadow, B, 0, stream_>>>(E);
         k_status<<<1, 1024, 0, stream_>>>(E, cur ^ 1);
         CK(cudaGetLastError());

@@ -97,10 +97,82 @@ __global__ void __launch_bounds__(kSchedThreads) k_schedule(EngineView E, const 
     }
 }
 
+// ------------------------------------------------------------------ spectral weights
+// Per-channel XYZ weights of a path's wavelengths: w_k = cmf(lam_k) *
+// (700-400)/yBarIntegral / N, so the pixel contribution of per-channel
+// radiance c is sum_k c_k w_k = sum_k singleLambdaXYZ(lam_k, c_k) / N
+// (code/Renderer.cpp:254-257, code/Includes/CIE.h:140-159).  Computed once
+// per vertex; RGB mode passes the channels through.
+struct XyzWeights {
+    float3 w[4];
+};
+// Kept out of line: seven double-precision exponentials per wavelength make
+// a large body, and one shared copy keeps k_shade's instruction footprint small.
+__device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale)
+{
+    XyzWeights W;
+    if (!spectral) {
+        W.w[0] = make_float3(1.f, 0.f, 0.f);
+        W.w[1] = make_float3(0.f, 1.f, 0.f);
+        W.w[2] = make_float3(0.f, 0.f, 1.f);
+        W.w[3] = make_float3(0.f, 0.f, 0.f);
+        return W;
+    }
+    for (int k = 0; k < 4; k++) {
+        if (k < nch) {
+            float3 c = cmf(lam[k]);
+            const float s = xyz_scale * wN;
+            W.w[k] = make_float3(c.x * s, c.y * s, c.z * s);
+        } else {
+            W.w[k] = make_float3(0.f, 0.f, 0.f);
+        }
+    }
+    return W;
+}
+// Packed layout of the weights in the path queue (see PathQueue::w).
+__device__ __forceinline__ void store_weights(const PathQueue& Q, int pos, const XyzWeights& W)
+{
+    Q.w[0][pos] = make_float4(W.w[0].x, W.w[0].y, W.w[0].z, W.w[1].x);
+    Q.w[1][pos] = make_float4(W.w[1].y, W.w[1].z, W.w[2].x, W.w[2].y);
+    Q.w[2][pos] = make_float4(W.w[2].z, W.w[3].x, W.w[3].y, W.w[3].z);
+}
+__device__ __forceinline__ XyzWeights load_weights(const PathQueue& Q, int pos)
+{
+    const float4 a = Q.w[0][pos], b = Q.w[1][pos], c = Q.w[2][pos];
+    XyzWeights W;
+    W.w[0] = make_float3(a.x, a.y, a.z);
+    W.w[1] = make_float3(a.w, b.x, b.y);
+    W.w[2] = make_float3(b.z, b.w, c.x);
+    W.w[3] = make_float3(c.y, c.z, c.w);
+    return W;
+}
+__device__ __forceinline__ XyzWeights rgb_weights()
+{
+    XyzWeights W;
+    W.w[0] = make_float3(1.f, 0.f, 0.f);
+    W.w[1] = make_float3(0.f, 1.f, 0.f);
+    W.w[2] = make_float3(0.f, 0.f, 1.f);
+    W.w[3] = make_float3(0.f, 0.f, 0.f);
+    return W;
+}
+
+__device__ __forceinline__ float3 apply_xyz(const XyzWeights& W, const float* c)
+{
+    float3 s = make_float3(0.f, 0.f, 0.f);
+    for (int k = 0; k < 4; k++) {
+        s.x += c[k] * W.w[k].x;
+        s.y += c[k] * W.w[k].y;
+        s.z += c[k] * W.w[k].z;
+    }
+    return s;
+}
+
+
 // ------------------------------------------------------------------ regen
 // Camera rays for the new paths (code/Renderer.cpp:190-239): pixel centre,
 // jitter when aa > 1, hero wavelength and its stratified companions.
-__global__ void k_regen(EngineView E, int cur)
+
+__global__ void k_regen(EngineView E, int cur, float xyz_scale)
 {
     __shared__ int s_base[kMaxActive];
     __shared__ int s_give[kMaxActive];
@@ -142,12 +214,23 @@ __global__ void k_regen(EngineView E, int cur)
         float3 d = make_float3(x * inv, y * inv, -inv);
         float lambda0 = 0.f;
         int nch = 4;
+        const int pos = base + i;
         if (R.flags & kReqSpectral) {
             float4 u = rand4(R, pixel, sample, 0, 255u, 0);
             lambda0 = 400.f + u.x * 300.f;
             nch = R.hero;
+            // hero wavelength and its stratified companions (code/Renderer.cpp:227-239)
+            float lam[4];
+            const float span = 300.f, stride_l = span / (float)nch;
+            lam[0] = lambda0;
+#pragma unroll
+            for (int k = 1; k < 4; k++) {
+                float l = lam[0] + stride_l * k;
+                if (l > 700.f) l -= span;
+                lam[k] = k < nch ? l : lam[0];
+            }
+            store_weights(Q, pos, xyz_weights(true, lam, nch, 1.f / (float)nch, xyz_scale));
         }
-        const int pos = base + i;
         Q.o[pos] = make_float4(R.cam_x, R.cam_y, R.cam_z, lambda0);
         Q.d[pos] = make_float4(d.x, d.y, d.z, __int_as_float(nch << 12));
         Q.tp[pos] = make_float4(1.f, 1.f, 1.f, 1.f);
@@ -196,52 +279,6 @@ __device__ __forceinline__ void add_xyz(double* acc, float3 c)
     atomicAdd(acc + 2, (double)c.z);
 }
 
-// Per-channel XYZ weights of a path's wavelengths: w_k = cmf(lam_k) *
-// (700-400)/yBarIntegral / N, so the pixel contribution of per-channel
-// radiance c is sum_k c_k w_k = sum_k singleLambdaXYZ(lam_k, c_k) / N
-// (code/Renderer.cpp:254-257, code/Includes/CIE.h:140-159).  Computed once
-// per vertex; RGB mode passes the channels through.
-struct XyzWeights {
-    float3 w[4];
-};
-// Kept out of line: seven double-precision exponentials per wavelength make
-// a large body, and one shared copy keeps k_shade's instruction footprint small.
-__device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale)
-{
-    XyzWeights W;
-    if (!spectral) {
-        W.w[0] = make_float3(1.f, 0.f, 0.f);
-        W.w[1] = make_float3(0.f, 1.f, 0.f);
-        W.w[2] = make_float3(0.f, 0.f, 1.f);
-        W.w[3] = make_float3(0.f, 0.f, 0.f);
-        return W;
-    }
-    for (int k = 0; k < 4; k++) {
-        if (k < nch) {
-            float3 c = cmf(lam[k]);
-            const float s = xyz_scale * wN;
-            W.w[k] = make_float3(c.x * s, c.y * s, c.z * s);
-        } else {
-            W.w[k] = make_float3(0.f, 0.f, 0.f);
-        }
-    }
-    return W;
-}
-__device__ __forceinline__ float3 apply_xyz(const XyzWeights& W, const float* c)
-{
-    float3 s = make_float3(0.f, 0.f, 0.f);
-    for (int k = 0; k < 4; k++) {
-        s.x += c[k] * W.w[k].x;
-        s.y += c[k] * W.w[k].y;
-        s.z += c[k] * W.w[k].z;
-    }
-    return s;
-}
-
-struct ShadeConst {
-    float xyz_scale;  // (700-400) / yBarIntegral
-};
-
 // ------------------------------------------------------------------ shade
 // Appends `count` records for the calling lane among the lanes that reach the
 // call together (divergent code): one atomic per coalesced group.
@@ -267,7 +304,7 @@ __device__ __forceinline__ int group_append(int* counter, int count)
 // The spectral product albedo * emission * XYZ weight is formed once per
 // vertex and light material, so each shadow sample only scales it by its
 // geometry term.
-__global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeConst K, int smem_mats)
+__global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int smem_mats)
 {
     extern __shared__ DMaterial s_mat[];
     const DMaterial* M = E.mats;
@@ -306,17 +343,17 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeCo
         double* acc = nullptr;
         float3 emit_xyz = make_float3(0, 0, 0);
         bool emit = false;
+        bool spec_path = false;
 
         if (live && (prim & kPrimKindMask) != kPrimNone) {
             const DRequest& R = E.reqs[slot];
             const DScene& S = E.scenes[R.scene];
             const bool spectral = (R.flags & kReqSpectral) != 0;
+            spec_path = spectral;
             // wavelengths carried by this path (code/Renderer.cpp:227-239)
             float lam[4];
             int nch = 3;
-            float wN = 1.f;
             if (spectral) {
-                wN = 1.f / (float)nHero;
                 if (single) {
                     lam[0] = lam[1] = lam[2] = lam[3] = o4.w;
                     nch = 1;
@@ -375,7 +412,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeCo
                 } else {
                     c[0] = tp[0] * m.emissive.x; c[1] = tp[1] * m.emissive.y; c[2] = tp[2] * m.emissive.z;
                 }
-                const XyzWeights W = xyz_weights(spectral, lam, nch, wN, K.xyz_scale);
+                const XyzWeights W = spectral ? load_weights(Q, i) : rgb_weights();
                 emit_xyz = apply_xyz(W, c);
                 emit = true;
             } else if (m.flags & kMatMetallic) {
@@ -436,6 +473,14 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeCo
                                 NQ.d[pos] = make_float4(bd.x, bd.y, bd.z, __int_as_float(fm));
                                 NQ.tp[pos] = make_float4(ftp, ftp, ftp, ftp);
                                 NQ.id[pos] = id;
+                                // the sub-path keeps wavelength k's weight alone
+                                const float4 wk = k == 0 ? Q.w[0][i]
+                                                : k == 1 ? make_float4(Q.w[0][i].w, Q.w[1][i].x, Q.w[1][i].y, 0.f)
+                                                : k == 2 ? make_float4(Q.w[1][i].z, Q.w[1][i].w, Q.w[2][i].x, 0.f)
+                                                         : make_float4(Q.w[2][i].y, Q.w[2][i].z, Q.w[2][i].w, 0.f);
+                                NQ.w[0][pos] = make_float4(wk.x, wk.y, wk.z, 0.f);
+                                NQ.w[1][pos] = make_float4(0.f, 0.f, 0.f, 0.f);
+                                NQ.w[2][pos] = make_float4(0.f, 0.f, 0.f, 0.f);
                             } else {
                                 atomicOr(&C->status, 2);
                             }
@@ -467,7 +512,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeCo
                 const float3 h1 = hc;
                 if (S.total_light_area > 0.f) {
                     const float scaleS = S.total_light_area * inv_pi / (float)R.shadow;
-                    const XyzWeights W = xyz_weights(spectral, lam, nch, wN, K.xyz_scale);
+                    const XyzWeights W = spectral ? load_weights(Q, i) : rgb_weights();
                     float tpal[4];
 #pragma unroll
                     for (int k = 0; k < 4; k++) tpal[k] = tp[k] * al[k];
@@ -589,6 +634,11 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, ShadeCo
                 NQ.d[pos] = make_float4(nd.x, nd.y, nd.z, __int_as_float(newMeta));
                 NQ.tp[pos] = ntp;
                 NQ.id[pos] = id;
+                if (spec_path) {
+                    NQ.w[0][pos] = Q.w[0][i];
+                    NQ.w[1][pos] = Q.w[1][i];
+                    NQ.w[2][pos] = Q.w[2][i];
+                }
             }
         }
         // path bookkeeping per request, one atomic per request per warp:

@@ -108,6 +108,10 @@ struct PathQueue {
     float4* d;     // direction, meta (bits): bounce | fork<<8 | single<<11 | n<<12
     float4* tp;    // throughput per channel
     int4* id;      // request slot, pixel, sample, unused
+    // XYZ weight of each carried wavelength, cmf(lambda_k) * 300/yBarIntegral / N
+    // (spectral paths only): w[0] = x0 y0 z0 x1, w[1] = y1 z1 x2 y2, w[2] = z2 x3 y3 z3.
+    // Computed once at raygen; a path's wavelengths never change.
+    float4* w[3];
 };
 
 struct ShadowQueue {
