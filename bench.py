@@ -53,6 +53,7 @@ def args_():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-profile", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-matched", action="store_true")
     p.add_argument("--queue", type=int, default=0, help="paths in flight (0: library default)")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-rate", type=float, default=200.0)
@@ -170,6 +171,93 @@ def reference_arm(a):
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"{rows} rows of each of the {a.renders} renders per step"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
+
+
+# ------------------------------------------------------------------ matched image error
+def matched_run(ctx, sids, stream, a, with_cpu):
+    """The Cornell configuration at matched image error: cornell.json at
+    256x256, depth 4, S = 4, hero-4 spectral, Reinhard.  The target error is
+    the RMSE of the reference CPU renderer's branched s = 16 image against a
+    4096-path converged image (both made by the reference itself,
+    tests/golden/converged_cornell256.npz).  spp* is the smallest paths per
+    pixel whose mean RMSE over 4 seeds reaches that target; the GPU then
+    renders W*H*spp* paths per image, plain (one render per launch sequence)
+    and batched (64 seeds in one wavefront).  The CPU time is the branched
+    s = 16 render on a row sample, all host threads, scaled to the image."""
+    import torch
+
+    from pcr_b200 import capi
+    fx = np.load(os.path.join(REPO, "tests", "golden", "converged_cornell256.npz"))
+    conv, eps = fx["image"].astype(np.float64), float(fx["branched_rmse"])
+    sid, W = sids["cornell"], 256
+
+    def desc(spp, seed):
+        return capi.render_desc(W, depth=4, samples=spp, shadow=4, spectral=True, seed=seed)
+
+    def rmse(spp, seed):
+        hdr, _, _ = ctx.render(sid, desc(spp, seed), want_rgb=False)
+        return float(np.sqrt(np.mean((hdr.astype(np.float64) - conv) ** 2)))
+
+    spp_star, err = None, None
+    for spp in range(1, 65):
+        err = float(np.mean([rmse(spp, 1 + k) for k in range(4)]))
+        if err <= eps:
+            spp_star = spp
+            break
+    if spp_star is None:
+        return {"target_rmse": eps, "spp_star": None, "note": "target not reached by 64 paths per pixel"}
+    paths = W * W * spp_star
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for k in range(3):
+        ctx.render(sid, desc(spp_star, 100 + k), want_hdr=False, want_rgb=False)
+    reps = 20
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for k in range(reps):
+        ctx.render(sid, desc(spp_star, 200 + k), want_hdr=False, want_rgb=False)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_s = e0.elapsed_time(e1) / 1e3 / reps
+    nb = 64
+
+    def batch(seed0):
+        ids = [ctx.submit(sid, desc(spp_star, seed0 + k)) for k in range(nb)]
+        ctx.run_until_idle()
+        for i in ids:
+            ctx.fetch(i, want_hdr=False, want_rgb=False)
+    batch(300)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    batch(400)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    batched_s = e0.elapsed_time(e1) / 1e3 / nb
+    out = {"config": "cornell.json 256x256, depth 4, S=4, hero-4 spectral, Reinhard",
+           "target_rmse": eps, "target": "reference CPU branched s=16 image vs 4096-path converged image",
+           "spp_star": spp_star, "gpu_rmse_at_spp_star": err, "paths_per_image": paths,
+           "plain_ms_per_image": plain_s * 1e3, "plain_paths_s": paths / plain_s,
+           "batched_ms_per_image": batched_s * 1e3, "batched_paths_s": paths / batched_s, "batched_images": nb}
+    if with_cpu:
+        try:
+            from oracle import ref
+            if ref.available():
+                sc = ref.load_scene(os.path.join(REPO, "tests", "golden", "scenes", "cornell.json"),
+                                    os.path.join(REPO, "tests", "golden"))
+                # four bands spread over the image, one row per host thread in each
+                band = min(W // 8, os.cpu_count() or 8)
+                o = ref.opts(W, depth=4, samples=16, shadow=4, spectral=True, seed=1)
+                secs = 0.0
+                for b in range(4):
+                    r0 = b * (W // 4) + (W // 8)
+                    secs += ref.render_hdr(sc, o, mode=0, threads=0, rows=(r0, r0 + band))[1]
+                t_img = secs * W / (4 * band)
+                out.update({"cpu_branched_s_per_image": t_img, "cpu_cores": os.cpu_count(),
+                            "cpu_sample": f"4 bands of {band} rows of the branched s=16 render, scaled to {W} rows",
+                            "cpu_equiv_paths_s": paths / t_img,
+                            "plain_over_cpu": t_img / plain_s, "batched_over_cpu": t_img / batched_s})
+        except Exception as e:  # reported, not fatal
+            out["cpu_error"] = str(e)
+    return out
 
 
 # ------------------------------------------------------------------ served stream
@@ -346,6 +434,11 @@ def main():
     if a.serve_requests > 0:
         serve = serve_run(ctx, sids, files, data, a)
 
+    # ---- Cornell configuration at matched image error
+    matched = None
+    if not a.no_matched:
+        matched = matched_run(ctx, sids, stream, a, with_cpu=(not a.no_cpu and rank == 0 and world == 1))
+
     # ---- CPU baseline (rank 0, N = 1): reference renderer on a row sample
     cpu = None
     if not a.no_cpu and rank == 0 and world == 1:
@@ -375,7 +468,7 @@ def main():
             "plain_value": plain, "batched_over_plain": (value / plain) if plain else None,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
-            "serve": serve,
+            "serve": serve, "matched_rmse": matched,
             "tuning": {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")},
         }
         print(json.dumps(out))

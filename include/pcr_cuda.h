@@ -228,6 +228,12 @@ pcr_status pcr_trace_closest(pcr_ctx *ctx, pcr_scene_id scene, const float *rays
  * per-ray counts of internal nodes visited and triangles tested (may be NULL). */
 pcr_status pcr_trace_bvh(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, int64_t n,
                          int32_t *tri_id, float *t, int32_t *counts);
+/* The shadow test of one light sample (code/Renderer.cpp:852-860) on caller
+ * rays: rays = n x (origin xyz, unit direction xyz), light_dist2 = squared
+ * distance to the light sample; blocked[i] = 1 when the closest hit is
+ * non-emissive and closer than light_dist2 - 1e-3 (compared in double). */
+pcr_status pcr_trace_shadow(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, const float *light_dist2,
+                            int64_t n, int32_t *blocked);
 /* Device evaluations of the FP32 stage functions on a wavelength / colour grid:
  * what 0 sigmoid fit at lambda (fit=4 floats) | 1 tabulated spectrum (61) |
  * 2 CIE xbar/ybar/zbar (3 out) | 3 singleLambdaXYZ(lambda, in[i]) (3 out) |

@@ -26,7 +26,7 @@ EXPORTS = [
     "pcr_fit_sigmoid", "pcr_lut_build", "pcr_scene_release", "pcr_scene_bytes", "pcr_render", "pcr_render_noalloc",
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
     "pcr_fetch", "pcr_cancel", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
-    "pcr_trace_closest", "pcr_trace_bvh", "pcr_eval_stage",
+    "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_eval_stage",
 ]
 
 
@@ -152,6 +152,7 @@ def load_library():
         "pcr_autotune": [P, ip, C.POINTER(RenderDesc), C.c_int32, ip],
         "pcr_trace_closest": [P, C.c_int32, fp, C.c_int64, ip, ip, fp],
         "pcr_trace_bvh": [P, C.c_int32, fp, C.c_int64, ip, fp, ip],
+        "pcr_trace_shadow": [P, C.c_int32, fp, fp, C.c_int64, ip],
         "pcr_eval_stage": [P, C.c_int32, fp, fp, C.c_int64, fp],
     }
     for name, args in sig.items():
@@ -396,6 +397,16 @@ class Context:
         cnt = np.zeros((n, 2), np.int32) if counts else None
         _check(self.L.pcr_trace_bvh(self.h, sid, _fp(r), n, _ip(tid), _fp(t), _ip(cnt) if counts else None))
         return (tid, t, cnt) if counts else (tid, t)
+
+    def trace_shadow(self, sid: int, rays: np.ndarray, light_dist2: np.ndarray) -> np.ndarray:
+        """Shadow test per ray (origin, unit direction) with its squared light
+        distance: 1 where blocked."""
+        r = np.ascontiguousarray(rays, np.float32)
+        d2 = np.ascontiguousarray(light_dist2, np.float32)
+        n = r.shape[0]
+        out = np.zeros(n, np.int32)
+        _check(self.L.pcr_trace_shadow(self.h, sid, _fp(r), _fp(d2), n, _ip(out)))
+        return out
 
     def eval_stage(self, what: int, inp: np.ndarray, params: np.ndarray | None = None) -> np.ndarray:
         x = np.ascontiguousarray(inp, np.float32)

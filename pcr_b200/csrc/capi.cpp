@@ -274,6 +274,15 @@ pcr_status pcr_trace_bvh(pcr_ctx* ctx, pcr_scene_id scene, const float* rays, in
     });
 }
 
+pcr_status pcr_trace_shadow(pcr_ctx* ctx, pcr_scene_id scene, const float* rays, const float* light_dist2, int64_t n,
+                            int32_t* blocked)
+{
+    return guard([&] {
+        if ((!rays || !light_dist2 || !blocked) && n > 0) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        E(ctx).trace_shadow(scene, rays, light_dist2, n, blocked);
+    });
+}
+
 pcr_status pcr_eval_stage(pcr_ctx* ctx, int32_t what, const float* params, const float* in, int64_t n, float* out)
 {
     return guard([&] {

@@ -78,7 +78,7 @@ __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, f
 {
     using namespace ex;
     const float kUp = 1.f + 9.5367431640625e-07f, kDown = 1.f - 9.5367431640625e-07f;  // 1 +- 2^-20
-    float4 nA = p.n_area;
+    float4 nA = p.n_emit;
     float3 N = make_float3(nA.x, nA.y, nA.z);
     float denom = dot(d, N);
     if (fabsf(denom) <= 1e-6f) return false;
@@ -92,7 +92,9 @@ __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, f
     if (tq > closest * kUp || tq < 1e-6f * kDown) return false;
     float t = div(num, denom);
     t0 = t;
-    if (t <= 1e-6f || t > closest) return false;
+    // every caller keeps a hit only when t < closest (first tested wins a
+    // tie), so t == closest is rejected here already
+    if (t <= 1e-6f || t >= closest) return false;
     float3 lh = sub3(add3(o, scale3(d, t)), po);
     float4 u = p.u_uu, v = p.v_vv;
     float a = dot(lh, make_float3(u.x, u.y, u.z));
@@ -161,12 +163,26 @@ __device__ __forceinline__ bool slab(float lx, float hx, float ly, float hy, flo
 
 struct TraceCounts { int nodes, tris; };
 
+// The shadow test's distance check (code/Renderer.cpp:852-860): a hit at t
+// blocks when lightDist2 - 1e-3 > |hit - origin|^2, the hit point and its
+// squared distance taken with the reference's float operations and the
+// comparison in double (`lim` = lightDist2 - 1e-3 in double).
+__device__ __forceinline__ bool blocks_at(float3 o, float3 d, float t, double lim)
+{
+    const float3 sh = make_float3(__fadd_rn(o.x, __fmul_rn(d.x, t)), __fadd_rn(o.y, __fmul_rn(d.y, t)),
+                                  __fadd_rn(o.z, __fmul_rn(d.z, t)));
+    const float3 dd = ex::sub3(sh, o);
+    return lim > (double)ex::dot(dd, dd);
+}
+
 // Closest hit over the 4-wide BVH (ordered traversal, stack in local memory).
 // `closest` comes in as the best t from spheres/planes.  Returns the leaf-order
-// triangle index or -1; t/u/v of the hit.
-template <bool kCount>
+// triangle index or -1; t/u/v of the hit.  With kAny (shadow rays over a
+// mesh without emissive triangles) it returns -2 as soon as a hit closer
+// than `closest` blocks (blocks_at with `lim`).
+template <bool kCount, bool kAny = false>
 __device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d, float& closest, float& hu, float& hv,
-                                            TraceCounts* cnt)
+                                            TraceCounts* cnt, double lim = 0.0)
 {
     if (S.n_nodes <= 0) return -1;
     float3 inv = make_float3(__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdiv_rn(1.f, d.z));
@@ -212,6 +228,7 @@ __device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d,
                 if (kCount) cnt->tris++;
                 float t, u, v;
                 if (tri_hit(a, b, c, o, d, closest, t, u, v)) {
+                    if (kAny && blocks_at(o, d, t, lim)) return -2;
                     closest = t;
                     hu = u;
                     hv = v;
@@ -221,6 +238,28 @@ __device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d,
         }
     }
     return best;
+}
+
+// Conservative ray-box test for a plane group.  The box is padded on the
+// host by well over the rounding error of a hit point, the segment end by
+// 1e-4 relative; direction components below 1e-30 count as zero (the ray
+// then moves less than the padding along that axis).  A false answer means
+// no plane of the group can be hit in (0, closest].
+__device__ __forceinline__ bool group_axis(float lo, float hi, float o, float d, float r, float& tmin, float& tmax)
+{
+    if (fabsf(d) < 1e-30f) return o >= lo && o <= hi;
+    const float t1 = (lo - o) * r, t2 = (hi - o) * r;
+    tmin = fmaxf(tmin, fminf(t1, t2));
+    tmax = fminf(tmax, fmaxf(t1, t2));
+    return true;
+}
+__device__ __forceinline__ bool group_may_hit(float4 lo, float4 hi, float3 o, float3 d, float3 rd, float closest)
+{
+    float tmin = 0.f, tmax = closest * 1.0001f + 1e-4f;
+    if (!group_axis(lo.x, hi.x, o.x, d.x, rd.x, tmin, tmax)) return false;
+    if (!group_axis(lo.y, hi.y, o.y, d.y, rd.y, tmin, tmax)) return false;
+    if (!group_axis(lo.z, hi.z, o.z, d.z, rd.z, tmin, tmax)) return false;
+    return tmin <= tmax;
 }
 
 // Renderer::sceneIntersect (code/Renderer.cpp:891-949): spheres, then planes
@@ -238,17 +277,85 @@ __device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, flo
             prim = kPrimSphere | (uint32_t)i;
         }
     }
-    for (int i = 0; i < S.n_planes; i++) {
-        float t0;
-        if (plane_hit(S.planes[i], o, d, closest, t0) && t0 < closest) {
-            closest = t0;
-            prim = kPrimPlane | (uint32_t)i;
+    // planes in order, a group's planes skipped together when the ray cannot
+    // reach the group's (padded) box before `closest`; skipping planes that
+    // cannot be hit leaves the closest hit and its tie order unchanged
+    const float3 rd = make_float3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    for (int g = 0; g < S.n_pgroups; g++) {
+        const float4 lo = S.pgroups[2 * g], hi = S.pgroups[2 * g + 1];
+        const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
+        if (count > 1 && !group_may_hit(lo, hi, o, d, rd, closest)) continue;
+        for (int i = first; i < first + count; i++) {
+            float t0;
+            if (plane_hit(S.planes[i], o, d, closest, t0) && t0 < closest) {
+                closest = t0;
+                prim = kPrimPlane | (uint32_t)i;
+            }
         }
     }
     int tri = bvh4_closest<false>(S, o, d, closest, hu, hv, nullptr);
     if (tri >= 0) prim = kPrimTri | (uint32_t)tri;
     t = closest;
     return prim;
+}
+
+// Shadow query with early exit: true when the closest hit of the segment
+// would block (non-emissive and closer than the light, code/Renderer.cpp:852-
+// 860).  The closest emissive sphere or plane is found first; nothing behind
+// it can block.  Then the other spheres, the non-emissive planes (their own
+// grouped copy) and the BVH are tested against that bound; a hit strictly in
+// front of the bound is non-emissive, so it either blocks (return at once) or
+// lies at the light and becomes the new bound.  A blocking hit found
+// this way implies the closest hit blocks as well (the squared distance grows
+// with t), so the answer is the closest-hit test's.  Scenes with emissive
+// triangles, or with more emissive spheres or planes than the scene record
+// lists, take the closest-hit route.
+__device__ __forceinline__ bool scene_blocked(const DScene& S, const DMaterial* mats, float3 o, float3 d, float tmax,
+                                              double lim)
+{
+    float t, hu, hv;
+    if (S.emissive_tris || S.n_emit_spheres < 0 || S.n_emit_planes < 0) {
+        t = FLT_MAX;
+        const uint32_t prim = scene_closest(S, o, d, tmax, t, hu, hv);
+        if ((prim & kPrimKindMask) == kPrimNone) return false;
+        const uint32_t kind = prim & kPrimKindMask, pidx = prim & kPrimIndexMask;
+        int mi;
+        if (kind == kPrimSphere) mi = S.spheres[pidx].mat.x;
+        else if (kind == kPrimPlane) mi = __float_as_int(S.planes[pidx].o_mat.w);
+        else mi = __float_as_int(S.tris[pidx].e1_mat.w);
+        if (mats[S.mat_base + mi].flags & kMatEmissive) return false;
+        return blocks_at(o, d, t, lim);
+    }
+    float bound = tmax;
+    for (int k = 0; k < S.n_emit_spheres; k++) {
+        float t0;
+        if (sphere_hit(S.spheres[S.emit_spheres[k]], o, d, t0) && t0 < bound) bound = t0;
+    }
+    for (int k = 0; k < S.n_emit_planes; k++) {
+        float t0;
+        if (plane_hit(S.planes[S.emit_planes[k]], o, d, bound, t0) && t0 < bound) bound = t0;
+    }
+    for (int i = 0; i < S.n_spheres; i++) {
+        float t0;
+        if (sphere_hit(S.spheres[i], o, d, t0) && t0 < bound) {
+            if (blocks_at(o, d, t0, lim)) return true;
+            bound = t0;
+        }
+    }
+    const float3 rd = make_float3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    for (int g = 0; g < S.n_sgroups; g++) {
+        const float4 lo = S.sgroups[2 * g], hi = S.sgroups[2 * g + 1];
+        const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
+        if (count > 1 && !group_may_hit(lo, hi, o, d, rd, bound)) continue;
+        for (int i = first; i < first + count; i++) {
+            float t0;
+            if (plane_hit(S.splanes[i], o, d, bound, t0) && t0 < bound) {
+                if (blocks_at(o, d, t0, lim)) return true;
+                bound = t0;
+            }
+        }
+    }
+    return bvh4_closest<false, true>(S, o, d, bound, hu, hv, nullptr, lim) == -2;
 }
 
 // ----------------------------------------------------------------- spectra

@@ -252,6 +252,76 @@ EngineView Engine::view() const
 }
 
 // ---------------------------------------------------------------- scenes
+// Splits the plane list into runs of consecutive planes, each run either one
+// plane tested directly or several tested behind one box test (a box
+// primitive's six faces), so the closest-hit loop skips a run the ray cannot
+// reach.  The split minimises an expected cost by dynamic programming over
+// run boundaries: a lone plane costs 1 test, a boxed run of k planes costs
+// 0.6 (the box test) + k * P(hit).  P(hit) for rays that mostly start inside
+// the scene is estimated as the run box's share of the whole plane set's
+// volume (the origin lies inside it) plus its share of the surface area.  The order of the planes, and so the reference's
+// first-tested-wins tie rule, is unchanged.  Boxes are padded by 1e-4 times
+// the scene's largest coordinate (at least 1e-4), far above the rounding
+// error of a computed hit point.
+static std::vector<float4> plane_groups(const pcr_plane* p, int n)
+{
+    struct Box {
+        float lo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, hi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+        void add(float x, float y, float z) {
+            const float v[3] = {x, y, z};
+            for (int k = 0; k < 3; k++) { lo[k] = std::min(lo[k], v[k]); hi[k] = std::max(hi[k], v[k]); }
+        }
+        void add(const Box& b) { add(b.lo[0], b.lo[1], b.lo[2]); add(b.hi[0], b.hi[1], b.hi[2]); }
+        double area() const {
+            const double x = hi[0] - lo[0], y = hi[1] - lo[1], z = hi[2] - lo[2];
+            return 2.0 * (x * y + y * z + z * x);
+        }
+        double volume() const {
+            return (double)(hi[0] - lo[0]) * (double)(hi[1] - lo[1]) * (double)(hi[2] - lo[2]);
+        }
+    };
+    std::vector<Box> b(n);
+    Box all;
+    float big = 1.f;
+    for (int i = 0; i < n; i++) {
+        const float* o = p[i].origin;
+        const float* u = p[i].u;
+        const float* v = p[i].v;
+        b[i].add(o[0], o[1], o[2]);
+        b[i].add(o[0] + u[0], o[1] + u[1], o[2] + u[2]);
+        b[i].add(o[0] + v[0], o[1] + v[1], o[2] + v[2]);
+        b[i].add(o[0] + u[0] + v[0], o[1] + u[1] + v[1], o[2] + u[2] + v[2]);
+        all.add(b[i]);
+        for (int k = 0; k < 3; k++) big = std::max(big, std::max(std::fabs(b[i].lo[k]), std::fabs(b[i].hi[k])));
+    }
+    const double total = std::max(all.area(), 1e-30), total_v = std::max(all.volume(), 1e-30);
+    // best[j]: cost of planes [0, j); from[j]: start of the last run
+    std::vector<double> best(n + 1, 0.0);
+    std::vector<int> from(n + 1, 0);
+    for (int j = 1; j <= n; j++) {
+        best[j] = best[j - 1] + 1.0;
+        from[j] = j - 1;
+        Box g = b[j - 1];
+        for (int i = j - 2; i >= 0 && j - i <= 64; i--) {
+            g.add(b[i]);
+            const double c = best[i] + 0.6 + (j - i) * std::min(1.0, g.area() / total + g.volume() / total_v);
+            if (c < best[j]) { best[j] = c; from[j] = i; }
+        }
+    }
+    std::vector<std::pair<int, int>> runs;
+    for (int j = n; j > 0; j = from[j]) runs.push_back({from[j], j});
+    std::reverse(runs.begin(), runs.end());
+    const float pad = 1e-4f * big;
+    std::vector<float4> out;
+    for (auto [i, j] : runs) {
+        Box g;
+        for (int k = i; k < j; k++) g.add(b[k]);
+        out.push_back(make_float4(g.lo[0] - pad, g.lo[1] - pad, g.lo[2] - pad, __int_as_float_host(i)));
+        out.push_back(make_float4(g.hi[0] + pad, g.hi[1] + pad, g.hi[2] + pad, __int_as_float_host(j - i)));
+    }
+    return out;
+}
+
 int Engine::upload_scene(const pcr_scene_desc& d)
 {
     std::lock_guard<std::mutex> g(run_mu_);
@@ -323,7 +393,7 @@ int Engine::upload_scene(const pcr_scene_desc& d)
         check_mat(p.mat, "plane");
         DPlane P;
         P.o_mat = make_float4(p.origin[0], p.origin[1], p.origin[2], __int_as_float_host(p.mat));
-        P.n_area = make_float4(p.n[0], p.n[1], p.n[2], p.area);
+        P.n_emit = make_float4(p.n[0], p.n[1], p.n[2], (e.mats[p.mat].flags & kMatEmissive) ? 1.f : 0.f);
         // u.dot(u) exactly as Plane::intersect computes it (code/Includes/Plane.h:46-47)
         float uu = p.u[0] * p.u[0] + p.u[1] * p.u[1] + p.u[2] * p.u[2];
         float vv = p.v[0] * p.v[0] + p.v[1] * p.v[1] + p.v[2] * p.v[2];
@@ -336,7 +406,7 @@ int Engine::upload_scene(const pcr_scene_desc& d)
         const pcr_sphere& s = d.spheres[i];
         check_mat(s.mat, "sphere");
         spheres[i].c_r = make_float4(s.center[0], s.center[1], s.center[2], s.radius);
-        spheres[i].mat = make_int4(s.mat, 0, 0, 0);
+        spheres[i].mat = make_int4(s.mat, (e.mats[s.mat].flags & kMatEmissive) ? 1 : 0, 0, 0);
     }
     auto to_dtri = [&](const pcr_triangle& t, int id) {
         DTri T;
@@ -350,11 +420,13 @@ int Engine::upload_scene(const pcr_scene_desc& d)
         T.e2_flags = make_float4(e2[0], e2[1], e2[2], __int_as_float_host(t.smooth ? 1 : 0));
         return T;
     };
+    int emissive_tris = 0;
     std::vector<DTri> dtris(d.n_triangles);
     std::vector<float4> tri_n((size_t)d.n_triangles * 3), tri_flat(d.n_triangles);
     for (int i = 0; i < d.n_triangles; i++) {
         check_mat(tris[i].mat, "triangle");
         dtris[i] = to_dtri(tris[i], ids[i]);
+        if (e.mats[tris[i].mat].flags & kMatEmissive) emissive_tris = 1;
         tri_n[i * 3 + 0] = make_float4(tris[i].n0[0], tris[i].n0[1], tris[i].n0[2], 0.f);
         tri_n[i * 3 + 1] = make_float4(tris[i].n1[0], tris[i].n1[1], tris[i].n1[2], 0.f);
         tri_n[i * 3 + 2] = make_float4(tris[i].n2[0], tris[i].n2[1], tris[i].n2[2], 0.f);
@@ -429,6 +501,32 @@ int Engine::upload_scene(const pcr_scene_desc& d)
     S.light_tris = dupload(ltris, e.allocs, bytes);
     S.light_flatn = dupload(lflat, e.allocs, bytes);
     S.light_cum = dupload(lcum, e.allocs, bytes);
+    const std::vector<float4> pgroups = plane_groups(d.planes, d.n_planes);
+    S.pgroups = dupload(pgroups, e.allocs, bytes);
+    S.n_pgroups = (int)pgroups.size() / 2;
+    std::vector<pcr_plane> lit_src;
+    std::vector<DPlane> splanes;
+    for (int i = 0; i < d.n_planes; i++)
+        if (planes[i].n_emit.w == 0.f) {
+            lit_src.push_back(d.planes[i]);
+            splanes.push_back(planes[i]);
+        }
+    const std::vector<float4> sgroups = plane_groups(lit_src.data(), (int)lit_src.size());
+    S.splanes = dupload(splanes, e.allocs, bytes);
+    S.sgroups = dupload(sgroups, e.allocs, bytes);
+    S.n_sgroups = (int)sgroups.size() / 2;
+    S.emissive_tris = emissive_tris;
+    S.n_emit_spheres = S.n_emit_planes = 0;
+    for (int i = 0; i < d.n_spheres; i++)
+        if (spheres[i].mat.y) {
+            if (S.n_emit_spheres >= 0 && S.n_emit_spheres < kMaxEmitPrims) S.emit_spheres[S.n_emit_spheres++] = i;
+            else S.n_emit_spheres = -1;
+        }
+    for (int i = 0; i < d.n_planes; i++)
+        if (planes[i].n_emit.w != 0.f) {
+            if (S.n_emit_planes >= 0 && S.n_emit_planes < kMaxEmitPrims) S.emit_planes[S.n_emit_planes++] = i;
+            else S.n_emit_planes = -1;
+        }
     S.n_planes = d.n_planes;
     S.n_spheres = d.n_spheres;
     S.n_nodes = (int)nodes4.size();
@@ -602,7 +700,7 @@ void Engine::launch_iteration(int cur, bool prof)
     if (prof) CK(cudaEventRecord(prof_ev_[2], stream_));
     k_extend<<<grid_extend_, B, 0, stream_>>>(E, cur);
     if (prof) CK(cudaEventRecord(prof_ev_[3], stream_));
-    k_shade<<<grid_shade_, B, shade_smem_, stream_>>>(E, cur, smem_mats_);
+    k_shade<<<grid_shade_, kShadeBlock, shade_smem_, stream_>>>(E, cur, smem_mats_);
     if (prof) CK(cudaEventRecord(prof_ev_[4], stream_));
     k_shadow<<<grid_shadow_, B, 0, stream_>>>(E);
     if (prof) CK(cudaEventRecord(prof_ev_[5], stream_));
@@ -635,7 +733,7 @@ void Engine::build_graph()
     CK(cudaFuncSetAttribute(k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(shade_smem_, 0)));
     grid_for((const void*)k_regen, B, 0, &grid_regen_);
     grid_for((const void*)k_extend, B, 0, &grid_extend_);
-    grid_for((const void*)k_shade, B, shade_smem_, &grid_shade_);
+    grid_for((const void*)k_shade, kShadeBlock, shade_smem_, &grid_shade_);
     grid_for((const void*)k_shadow, B, 0, &grid_shadow_);
     if (graph_exec_) {
         cudaGraphExecDestroy(graph_exec_);
@@ -1167,14 +1265,14 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     int g_regen, g_extend, g_shade, g_shadow;
     grid_for((const void*)k_regen, B, 0, &g_regen);
     grid_for((const void*)k_extend, B, 0, &g_extend);
-    grid_for((const void*)k_shade, B, smem, &g_shade);
+    grid_for((const void*)k_shade, kShadeBlock, smem, &g_shade);
     grid_for((const void*)k_shadow, B, 0, &g_shadow);
     int cur = 0;
     auto iteration = [&]() {
         k_schedule<<<1, kSchedThreads, 0, stream_>>>(E, params, cur);
         k_regen<<<g_regen, B, 0, stream_>>>(E, cur, xyz_scale_);
         k_extend<<<g_extend, B, 0, stream_>>>(E, cur);
-        k_shade<<<g_shade, B, smem, stream_>>>(E, cur, smem_mats);
+        k_shade<<<g_shade, kShadeBlock, smem, stream_>>>(E, cur, smem_mats);
         k_shadow<<<g_shadow, B, 0, stream_>>>(E);
         k_status<<<1, 1024, 0, stream_>>>(E, cur ^ 1);
         CK(cudaGetLastError());
@@ -1232,6 +1330,30 @@ void Engine::trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_
     CK(cudaFreeAsync(d_prim, stream_));
     CK(cudaFreeAsync(d_t, stream_));
     if (d_cnt) CK(cudaFreeAsync(d_cnt, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::trace_shadow(int scene, const float* rays, const float* dist2, int64_t n, int32_t* blocked)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    if (scene < 0 || scene >= (int)scenes_.size() || !scenes_[scene].live) throw PcrError(PCR_ERR_NOT_FOUND, "unknown scene");
+    if (n <= 0) return;
+    float *d_rays = nullptr, *d_d2 = nullptr;
+    int* d_b = nullptr;
+    CK(cudaMallocAsync(&d_rays, n * 6 * sizeof(float), stream_));
+    CK(cudaMallocAsync(&d_d2, n * sizeof(float), stream_));
+    CK(cudaMallocAsync(&d_b, n * sizeof(int), stream_));
+    CK(cudaMemcpyAsync(d_rays, rays, n * 6 * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    CK(cudaMemcpyAsync(d_d2, dist2, n * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    int grid = 0;
+    grid_for((const void*)k_trace_shadow, 128, 0, &grid);
+    k_trace_shadow<<<grid, 128, 0, stream_>>>(d_scenes_ + scene, d_mats_, d_rays, d_d2, n, d_b);
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(blocked, d_b, n * sizeof(int), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaFreeAsync(d_rays, stream_));
+    CK(cudaFreeAsync(d_d2, stream_));
+    CK(cudaFreeAsync(d_b, stream_));
     CK(cudaStreamSynchronize(stream_));
 }
 

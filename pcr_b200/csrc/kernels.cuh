@@ -156,15 +156,38 @@ __device__ __forceinline__ XyzWeights rgb_weights()
     return W;
 }
 
-__device__ __forceinline__ float3 apply_xyz(const XyzWeights& W, const float* c)
+__device__ __forceinline__ float3 apply_xyz(const XyzWeights& W, float4 c)
 {
     float3 s = make_float3(0.f, 0.f, 0.f);
-    for (int k = 0; k < 4; k++) {
-        s.x += c[k] * W.w[k].x;
-        s.y += c[k] * W.w[k].y;
-        s.z += c[k] * W.w[k].z;
-    }
+    s.x += c.x * W.w[0].x; s.y += c.x * W.w[0].y; s.z += c.x * W.w[0].z;
+    s.x += c.y * W.w[1].x; s.y += c.y * W.w[1].y; s.z += c.y * W.w[1].z;
+    s.x += c.z * W.w[2].x; s.y += c.z * W.w[2].y; s.z += c.z * W.w[2].z;
+    s.x += c.w * W.w[3].x; s.y += c.w * W.w[3].y; s.z += c.w * W.w[3].z;
     return s;
+}
+
+__device__ __forceinline__ float comp4(float4 v, int k) { return k == 0 ? v.x : k == 1 ? v.y : k == 2 ? v.z : v.w; }
+__device__ __forceinline__ float4 mul4(float4 a, float4 b) { return make_float4(a.x * b.x, a.y * b.y, a.z * b.z, a.w * b.w); }
+__device__ __forceinline__ float4 rgb4(float4 c) { return make_float4(c.x, c.y, c.z, 0.f); }
+
+// A material spectrum at the four carried wavelengths (Material::albedoAt /
+// emissiveAt, code/Includes/Material.h:92-101).  Kept out of line: one copy
+// of the sigmoid / table code instead of one per call site keeps k_shade's
+// instruction footprint small.
+__device__ __noinline__ float4 spec4(const DMaterial& m, int emissive, float4 lam)
+{
+    const bool tab = (m.flags & (emissive ? kMatTabE : kMatTabA)) != 0;
+    const float* table = emissive ? m.tabE : m.tabA;
+    const float4 fit = emissive ? m.efit : m.afit;
+    float v[4];
+    const float l[4] = {lam.x, lam.y, lam.z, lam.w};
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        float x = tab ? spectrum_lerp(table, l[k]) : sigmoid_fit(fit, l[k]);
+        if (!emissive && !tab && x > 1.f) x = 1.f;
+        v[k] = x;
+    }
+    return make_float4(v[0], v[1], v[2], v[3]);
 }
 
 
@@ -239,8 +262,13 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
 }
 
 // ------------------------------------------------------------------ extend
+// The trace kernels are latency-bound (dependent IEEE arithmetic, scattered
+// scene loads): their register budget is capped at 64 per thread (blocks of
+// up to 256, 4 per SM) so 32 or more warps stay resident per SM.
+constexpr int kTraceMaxBlock = 256, kTraceMinBlocks = 4;
+
 // Closest hit for every queued path (trace_closest).
-__global__ void k_extend(EngineView E, int cur)
+__global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(EngineView E, int cur)
 {
     const Counters* C = E.cnt;
     const int n = min(C->queue_n[cur], E.queue_cap);
@@ -293,6 +321,10 @@ __device__ __forceinline__ int group_append(int* counter, int count)
     return g.shfl(base, 0) + ex;
 }
 
+// k_shade's block shape is fixed: its register budget (launch bounds) is
+// set for 128-thread blocks, 5 per SM.
+constexpr int kShadeBlock = 128;
+
 // Per-path shading of the hit found by k_extend (code/Renderer.cpp:656-889
 // with samples = 1, the GPU's paths-per-pixel estimator): emission,
 // mirror, dielectric (with the 4-way hero fork at dispersive glass),
@@ -304,7 +336,11 @@ __device__ __forceinline__ int group_append(int* counter, int count)
 // The spectral product albedo * emission * XYZ weight is formed once per
 // vertex and light material, so each shadow sample only scales it by its
 // geometry term.
-__global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int smem_mats)
+//
+// Per-channel values live in float4 registers (no per-thread arrays, so no
+// local memory); channels a path does not carry have zero XYZ weight, so
+// they are evaluated but contribute nothing.
+__global__ void __launch_bounds__(kShadeBlock, 5) k_shade(EngineView E, int cur, int smem_mats)
 {
     extern __shared__ DMaterial s_mat[];
     const DMaterial* M = E.mats;
@@ -351,27 +387,20 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
             const bool spectral = (R.flags & kReqSpectral) != 0;
             spec_path = spectral;
             // wavelengths carried by this path (code/Renderer.cpp:227-239)
-            float lam[4];
-            int nch = 3;
+            float4 lam4 = make_float4(0.f, 0.f, 0.f, 0.f);
             if (spectral) {
+                const float l0 = o4.w;
                 if (single) {
-                    lam[0] = lam[1] = lam[2] = lam[3] = o4.w;
-                    nch = 1;
+                    lam4 = make_float4(l0, l0, l0, l0);
                 } else {
                     const float span = 300.f, stride_l = span / (float)nHero;
-                    lam[0] = o4.w;
-#pragma unroll
-                    for (int k = 1; k < 4; k++) {
-                        float l = lam[0] + stride_l * k;
-                        if (l > 700.f) l -= span;
-                        lam[k] = k < nHero ? l : lam[0];
-                    }
-                    nch = nHero;
+                    float l1 = l0 + stride_l * 1, l2 = l0 + stride_l * 2, l3 = l0 + stride_l * 3;
+                    if (l1 > 700.f) l1 -= span;
+                    if (l2 > 700.f) l2 -= span;
+                    if (l3 > 700.f) l3 -= span;
+                    lam4 = make_float4(l0, 1 < nHero ? l1 : l0, 2 < nHero ? l2 : l0, 3 < nHero ? l3 : l0);
                 }
-            } else {
-                lam[0] = lam[1] = lam[2] = lam[3] = 0.f;
             }
-            const float tp[4] = {tp4.x, tp4.y, tp4.z, tp4.w};
             acc = R.accum + (size_t)id.y * 3;
             const float3 o = xyz(o4), d = xyz(d4);
             const float t = h.x;
@@ -385,7 +414,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                 N = f3mul(v, rsqrtf(f3dot(v, v)));
                 mi = S.spheres[pidx].mat.x;
             } else if (kind == kPrimPlane) {
-                const float4 na = S.planes[pidx].n_area;
+                const float4 na = S.planes[pidx].n_emit;
                 N = make_float3(na.x, na.y, na.z);
                 mi = __float_as_int(S.planes[pidx].o_mat.w);
             } else {
@@ -406,12 +435,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
             const DMaterial& m = M[S.mat_base + mi];
             const bool last = bounce + 1 >= R.depth;
             if (m.flags & kMatEmissive) {
-                float c[4] = {0.f, 0.f, 0.f, 0.f};
-                if (spectral) {
-                    for (int k = 0; k < nch; k++) c[k] = tp[k] * emissive_at(m, lam[k]);
-                } else {
-                    c[0] = tp[0] * m.emissive.x; c[1] = tp[1] * m.emissive.y; c[2] = tp[2] * m.emissive.z;
-                }
+                const float4 c = mul4(tp4, spectral ? spec4(m, 1, lam4) : rgb4(m.emissive));
                 const XyzWeights W = spectral ? load_weights(Q, i) : rgb_weights();
                 emit_xyz = apply_xyz(W, c);
                 emit = true;
@@ -420,11 +444,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                     const float cosI = -f3dot(d, N);
                     nd = f3add(d, f3mul(N, 2.f * cosI));
                     no = f3add(hit, f3mul(N, 1e-3f));
-                    if (spectral)
-                        ntp = make_float4(tp[0] * albedo_at(m, lam[0]), tp[1] * albedo_at(m, lam[1]),
-                                          tp[2] * albedo_at(m, lam[2]), tp[3] * albedo_at(m, lam[3]));
-                    else
-                        ntp = make_float4(tp[0] * m.albedo.x, tp[1] * m.albedo.y, tp[2] * m.albedo.z, 0.f);
+                    ntp = mul4(tp4, spectral ? spec4(m, 0, lam4) : rgb4(m.albedo));
                     cont = true;
                 }
             } else if (m.flags & kMatTransparent) {
@@ -433,20 +453,22 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                     const bool disperse = spectral && m.cauchyB != 0.f && !single && nHero > 1;
                     const int ways = disperse ? nHero : 1;
                     const float4 coins = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 63u);
+                    const float4 alg = spectral ? spec4(m, 0, lam4) : rgb4(m.albedo);
                     int fpos = 0;
                     if (disperse) {
                         fpos = group_append(&C->queue_n[cur ^ 1], ways);
                         forked = ways;
                     }
                     for (int k = 0; k < ways; k++) {
+                        const float lk = comp4(lam4, k);
                         float ior = m.ior;
                         if (spectral && m.cauchyB != 0.f && (disperse || single))
-                            ior = m.ior + m.cauchyB * 1e4f / (lam[k] * lam[k]);  // Optics::cauchyIor
+                            ior = m.ior + m.cauchyB * 1e4f / (lk * lk);  // Optics::cauchyIor
                         // Optics::dielectricBounce (code/Includes/Optics.h:59-82)
                         const float n1 = entering ? 1.f : ior, n2 = entering ? ior : 1.f;
                         const float eta = n1 / n2;
                         const float sinT2 = eta * eta * (1.f - cosI * cosI);
-                        const float u = k == 0 ? coins.x : (k == 1 ? coins.y : (k == 2 ? coins.z : coins.w));
+                        const float u = comp4(coins, k);
                         float3 bd, bo;
                         bool refl = sinT2 >= 1.f;
                         if (!refl) {
@@ -467,17 +489,18 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                             // sub-path k carries wavelength k alone (code/Renderer.cpp:736-753)
                             const int pos = fpos + k;
                             if (pos < E.queue_cap) {
-                                const float ftp = tp[k] * albedo_at(m, lam[k]);
+                                const float ftp = comp4(tp4, k) * comp4(alg, k);
                                 const int fm = (bounce + 1) | ((k + 1) << 8) | (1 << 11) | (nHero << 12);
-                                NQ.o[pos] = make_float4(bo.x, bo.y, bo.z, lam[k]);
+                                NQ.o[pos] = make_float4(bo.x, bo.y, bo.z, lk);
                                 NQ.d[pos] = make_float4(bd.x, bd.y, bd.z, __int_as_float(fm));
                                 NQ.tp[pos] = make_float4(ftp, ftp, ftp, ftp);
                                 NQ.id[pos] = id;
                                 // the sub-path keeps wavelength k's weight alone
-                                const float4 wk = k == 0 ? Q.w[0][i]
-                                                : k == 1 ? make_float4(Q.w[0][i].w, Q.w[1][i].x, Q.w[1][i].y, 0.f)
-                                                : k == 2 ? make_float4(Q.w[1][i].z, Q.w[1][i].w, Q.w[2][i].x, 0.f)
-                                                         : make_float4(Q.w[2][i].y, Q.w[2][i].z, Q.w[2][i].w, 0.f);
+                                const float4 w0 = Q.w[0][i], w1 = Q.w[1][i], w2 = Q.w[2][i];
+                                const float3 wk = k == 0 ? make_float3(w0.x, w0.y, w0.z)
+                                                : k == 1 ? make_float3(w0.w, w1.x, w1.y)
+                                                : k == 2 ? make_float3(w1.z, w1.w, w2.x)
+                                                         : make_float3(w2.y, w2.z, w2.w);
                                 NQ.w[0][pos] = make_float4(wk.x, wk.y, wk.z, 0.f);
                                 NQ.w[1][pos] = make_float4(0.f, 0.f, 0.f, 0.f);
                                 NQ.w[2][pos] = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -490,22 +513,13 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                         }
                     }
                     if (!disperse) {
-                        if (spectral)
-                            ntp = make_float4(tp[0] * albedo_at(m, lam[0]), tp[1] * albedo_at(m, lam[1]),
-                                              tp[2] * albedo_at(m, lam[2]), tp[3] * albedo_at(m, lam[3]));
-                        else
-                            ntp = make_float4(tp[0] * m.albedo.x, tp[1] * m.albedo.y, tp[2] * m.albedo.z, 0.f);
+                        ntp = mul4(tp4, alg);
                         cont = true;
                     }
                 }
             } else {
                 // diffuse
-                float al[4] = {0.f, 0.f, 0.f, 0.f};
-                if (spectral) {
-                    for (int k = 0; k < nch; k++) al[k] = albedo_at(m, lam[k]);
-                } else {
-                    al[0] = m.albedo.x; al[1] = m.albedo.y; al[2] = m.albedo.z;
-                }
+                const float4 al = spectral ? spec4(m, 0, lam4) : rgb4(m.albedo);
                 // indirect origin: hit moved once by 1e-3*N (the reference's
                 // mutating `hit + N * 1e-3`, code/Renderer.cpp:782 with samples = 1)
                 float3 hc = f3add(hit, f3mul(N, 1e-3f));
@@ -513,9 +527,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                 if (S.total_light_area > 0.f) {
                     const float scaleS = S.total_light_area * inv_pi / (float)R.shadow;
                     const XyzWeights W = spectral ? load_weights(Q, i) : rgb_weights();
-                    float tpal[4];
-#pragma unroll
-                    for (int k = 0; k < 4; k++) tpal[k] = tp[k] * al[k];
+                    const float4 tpal = mul4(tp4, al);
                     int cached = -1;
                     float3 V = make_float3(0.f, 0.f, 0.f);
                     int spos = group_append(&C->shadow_n, R.shadow);
@@ -576,13 +588,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                         if (lm != cached) {
                             // spectral product of this light material, once per vertex
                             const DMaterial& lmat = M[S.mat_base + lm];
-                            float c[4] = {0.f, 0.f, 0.f, 0.f};
-                            if (spectral) {
-                                for (int k = 0; k < nch; k++) c[k] = tpal[k] * emissive_at(lmat, lam[k]);
-                            } else {
-                                c[0] = tpal[0] * lmat.emissive.x; c[1] = tpal[1] * lmat.emissive.y;
-                                c[2] = tpal[2] * lmat.emissive.z;
-                            }
+                            const float4 c = mul4(tpal, spectral ? spec4(lmat, 1, lam4) : rgb4(lmat.emissive));
                             V = f3mul(apply_xyz(W, c), scaleS);
                             cached = lm;
                         }
@@ -601,7 +607,7 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                 bool survive = !last;
                 float rr_scale = 1.f;
                 if (survive && (R.flags & kReqRussian) && bounce >= 1) {
-                    float pr = spectral ? al[0] : fmaxf(fmaxf(al[0], al[1]), al[2]);
+                    float pr = spectral ? al.x : fmaxf(fmaxf(al.x, al.y), al.z);
                     pr = fminf(0.95f, fmaxf(0.05f, pr));
                     if (r0.w > pr) survive = false;
                     else rr_scale = 1.f / pr;
@@ -616,8 +622,8 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
                     }
                     nd = hemisphere(N, r1, r2);
                     no = h1;
-                    ntp = make_float4(tp[0] * al[0] * rr_scale, tp[1] * al[1] * rr_scale, tp[2] * al[2] * rr_scale,
-                                      tp[3] * al[3] * rr_scale);
+                    ntp = make_float4(tp4.x * al.x * rr_scale, tp4.y * al.y * rr_scale, tp4.z * al.z * rr_scale,
+                                      tp4.w * al.w * rr_scale);
                     cont = true;
                 }
             }
@@ -652,11 +658,12 @@ __global__ void __launch_bounds__(128, 5) k_shade(EngineView E, int cur, int sme
 }
 
 // ------------------------------------------------------------------ shadow
-// Shadow-ray test (code/Renderer.cpp:852-860): a closest-hit query bounded by
-// the light distance; the sample is blocked when the closest hit lies
-// closer than lightDist2 - 1e-3 (compared in double, as the reference's
-// double literal promotes it) and is not emissive.
-__global__ void k_shadow(EngineView E)
+// Shadow-ray test (code/Renderer.cpp:852-860): blocked when the closest hit
+// within the light distance is non-emissive and closer than lightDist2 -
+// 1e-3 (compared in double, as the reference's double literal promotes it);
+// scene_blocked answers it with an early exit.  Lit samples add their XYZ
+// contribution to the pixel's FP64 accumulator.
+__global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_shadow(EngineView E)
 {
     Counters* C = E.cnt;
     const int n = min(C->shadow_n, E.shadow_cap);
@@ -670,26 +677,11 @@ __global__ void k_shadow(EngineView E)
         const DRequest& R = E.reqs[slot];
         const DScene& S = E.scenes[R.scene];
         const float d2 = o.w;
+        // a hit beyond the light cannot block: bound the query just past it
         const float tmax = sqrtf(d2) * 1.0001f + 1e-4f;
-        float t = FLT_MAX, u, v;
-        const float3 so = xyz(o), wi = xyz(d);
-        const uint32_t prim = scene_closest(S, so, wi, tmax, t, u, v);
         mine++;
-        bool lit = true;
-        if ((prim & kPrimKindMask) != kPrimNone) {
-            const float3 sh = make_float3(__fadd_rn(so.x, __fmul_rn(wi.x, t)), __fadd_rn(so.y, __fmul_rn(wi.y, t)),
-                                          __fadd_rn(so.z, __fmul_rn(wi.z, t)));
-            const float3 dd = ex::sub3(sh, so);
-            const float dist2 = ex::dot(dd, dd);
-            int mi;
-            const uint32_t kind = prim & kPrimKindMask, pidx = prim & kPrimIndexMask;
-            if (kind == kPrimSphere) mi = S.spheres[pidx].mat.x;
-            else if (kind == kPrimPlane) mi = __float_as_int(S.planes[pidx].o_mat.w);
-            else mi = __float_as_int(S.tris[pidx].e1_mat.w);
-            const bool em = (E.mats[S.mat_base + mi].flags & kMatEmissive) != 0;
-            if ((double)d2 - 1e-3 > (double)dist2 && !em) lit = false;
-        }
-        if (lit) add_xyz(R.accum + (size_t)__float_as_int(d.w) * 3, make_float3(c.x, c.y, c.z));
+        if (!scene_blocked(S, E.mats, xyz(o), xyz(d), tmax, (double)d2 - 1e-3))
+            add_xyz(R.accum + (size_t)__float_as_int(d.w) * 3, make_float3(c.x, c.y, c.z));
     }
     for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, off);
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&C->shadow_rays, mine);
@@ -773,6 +765,20 @@ __global__ void k_trace_rays(const DScene* scene, const DMaterial* mats, const f
             prim_out[i] = (int)code;
             t_out[i] = kind ? t : 0.f;
         }
+    }
+}
+
+// The shadow test of k_shadow on caller rays (origin, unit direction) with
+// their squared light distances: 1 when blocked.
+__global__ void k_trace_shadow(const DScene* scene, const DMaterial* mats, const float* __restrict__ rays,
+                               const float* __restrict__ dist2, long long n, int* blocked)
+{
+    const DScene& S = *scene;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float3 o = make_float3(rays[i * 6], rays[i * 6 + 1], rays[i * 6 + 2]);
+        const float3 d = make_float3(rays[i * 6 + 3], rays[i * 6 + 4], rays[i * 6 + 5]);
+        const float d2 = dist2[i];
+        blocked[i] = scene_blocked(S, mats, o, d, sqrtf(d2) * 1.0001f + 1e-4f, (double)d2 - 1e-3) ? 1 : 0;
     }
 }
 

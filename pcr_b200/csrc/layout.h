@@ -14,6 +14,7 @@ constexpr int kSpecN = 61;          // 400..700 nm at 5 nm (code/Includes/Spectr
 constexpr int kMaxActive = 1024;    // request slots in flight at once
 constexpr int kMaxShadow = 64;      // shadow rays per diffuse vertex the kernels accept
 constexpr int kStackSize = 64;      // BVH4 traversal stack entries per ray
+constexpr int kMaxEmitPrims = 4;    // emissive spheres / planes listed per scene
 
 // Primitive code in a hit record: kind in the top two bits.
 constexpr uint32_t kPrimNone = 0u;
@@ -40,14 +41,14 @@ struct alignas(16) DMaterial {
 // Parallelogram (code/Includes/Plane.h): 4 x 16 B.
 struct alignas(16) DPlane {
     float4 o_mat;   // origin, matIdx (bits)
-    float4 n_area;  // unit normal, area
+    float4 n_emit;  // unit normal, 1 when the plane's material is emissive (else 0)
     float4 u_uu;    // u, dot(u,u)
     float4 v_vv;    // v, dot(v,v)
 };
 
 struct alignas(16) DSphere {
     float4 c_r;     // centre, radius
-    int4 mat;       // matIdx, pad
+    int4 mat;       // matIdx, 1 when the material is emissive (else 0), pad
 };
 
 // Triangle for Moller-Trumbore (code/Includes/Triangle.h:53-92): v0, e1 = v1-v0,
@@ -85,7 +86,21 @@ struct DScene {
     const DTri* light_tris;
     const float4* light_flatn;
     const float* light_cum;
-    int n_planes, n_spheres, n_nodes, n_tris, n_lights, mat_base, n_mats;
+    // Plane groups: runs of consecutive planes (a box's six faces) behind one
+    // conservative bounding-box test.  2 words per group: (lo, first plane),
+    // (hi, plane count); a group of one plane has no box test.
+    const float4* pgroups;
+    // The non-emissive planes again, grouped the same way, for the shadow
+    // query (which tests emissive planes separately and needs no tie order).
+    const DPlane* splanes;
+    const float4* sgroups;
+    int n_planes, n_spheres, n_nodes, n_tris, n_lights, mat_base, n_mats, n_pgroups;
+    int n_sgroups;
+    int emissive_tris;        // 1 when any triangle's material is emissive
+    // Emissive spheres and planes (indices), for the shadow query's first
+    // pass; n_emit_* = -1 when a scene has more than kMaxEmitPrims of a kind.
+    int n_emit_spheres, n_emit_planes;
+    int emit_spheres[kMaxEmitPrims], emit_planes[kMaxEmitPrims];
     float total_light_area;
 };
 

@@ -63,6 +63,60 @@ def test_trace_closest_bit_exact(ctx, O, name):
     ctx.release_scene(sid)
 
 
+def _shadow_rays(osc, n, seed):
+    """Shadow segments as k_shade makes them: origins in the box, targets half
+    on the scene's light planes, half anywhere in the box; direction
+    Li * rsqrt(|Li|^2) and |Li|^2 in float32."""
+    rng = np.random.default_rng(seed)
+    o = box_rays(n, seed)[:, :3]
+    lp = [L for L in osc.lights if L[0] == 0] if hasattr(osc, "lights") else []
+    P = box_rays(n, seed + 1)[:, :3]
+    if lp:
+        k = rng.integers(0, len(lp), n)
+        a, b = rng.uniform(size=n), rng.uniform(size=n)
+        for j, L in enumerate(lp):
+            pl = L[1]
+            sel = (k == j) & (np.arange(n) < n // 2)
+            P[sel] = (np.asarray(pl.origin, np.float32) + np.asarray(pl.u, np.float32) * a[sel, None]
+                      + np.asarray(pl.v, np.float32) * b[sel, None])
+    Li = (P - o).astype(np.float32)
+    d2 = (Li[:, 0] * Li[:, 0] + Li[:, 1] * Li[:, 1] + Li[:, 2] * Li[:, 2]).astype(np.float32)
+    ok = d2 > 1e-6
+    d = Li[ok] / np.sqrt(d2[ok])[:, None]
+    return np.concatenate([o[ok], d], 1).astype(np.float32), d2[ok]
+
+
+def _oracle_blocked(O, osc, rays, d2):
+    """code/Renderer.cpp:852-860 on the oracle: closest hit (reference
+    arithmetic), blocked when non-emissive and |hit - o|^2 < lightDist2 - 1e-3."""
+    mat, hn = O.scene_intersect(osc, rays)
+    emis = np.array([max(m.emissive) > 0 for m in osc.materials] + [False])
+    dd = (hn[:, :3] - rays[:, :3]).astype(np.float32)
+    dist2 = ((dd[:, 0] * dd[:, 0] + dd[:, 1] * dd[:, 1]).astype(np.float32) + dd[:, 2] * dd[:, 2]).astype(np.float32)
+    lim = d2.astype(np.float64) - 1e-3
+    blocked = (mat >= 0) & ~emis[mat] & (lim > dist2.astype(np.float64))
+    marginal = np.abs(lim - dist2) <= 1e-5 * np.maximum(d2, 1.0)
+    return blocked, marginal
+
+
+@pytest.mark.parametrize("name", PLANE_SCENES)
+def test_shadow_test_matches_oracle(ctx, O, name):
+    """k_shadow's early-exit query answers as the reference's closest-hit
+    shadow test does, except where the hit lies at the light distance within
+    rounding."""
+    sid = ctx.load_scene_json(scene_path(name), GOLDEN)
+    osc = O.load_scene(scene_path(name), GOLDEN)
+    rays, d2 = _shadow_rays(osc, 200_000, sum(name.encode()) + 5)
+    got = ctx.trace_shadow(sid, rays, d2).astype(bool)
+    want, marginal = _oracle_blocked(O, osc, rays, d2)
+    bad = (got != want) & ~marginal
+    assert bad.sum() == 0, f"{bad.sum()} shadow decisions differ ({(got != want).sum()} incl. marginal)"
+    assert want.mean() < 0.99
+    if name == "cornell":   # two boxes: a fair share of segments is blocked
+        assert want.mean() > 0.05
+    ctx.release_scene(sid)
+
+
 def _oracle_bvh_query(O, nodes, arr, rays, chunks=64):
     parts = np.array_split(np.arange(rays.shape[0]), chunks)
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
@@ -115,6 +169,20 @@ def test_bvh_hit_ids_10m_rays(ctx, O, mesh):
     bad = diff & ~ties
     assert bad.sum() == 0, f"{bad.sum()} id mismatches outside t-ties ({diff.sum()} total, {(gid >= 0).sum()} hits)"
     assert (gid >= 0).sum() > n // 20
+
+
+def test_shadow_test_matches_oracle_on_mesh(ctx, O, mesh):
+    """The early-exit shadow query through the 4-wide BVH (a blocking
+    triangle ends the walk) against the oracle's closest-hit test."""
+    from pcr_b200 import workloads
+    path = workloads.mesh_scene(59, 1)
+    osc = O.load_scene(path, GOLDEN)
+    rays, d2 = _shadow_rays(osc, 100_000, 41)
+    got = ctx.trace_shadow(mesh["sid"], rays, d2).astype(bool)
+    want, marginal = _oracle_blocked(O, osc, rays, d2)
+    bad = (got != want) & ~marginal
+    assert bad.sum() == 0, f"{bad.sum()} shadow decisions differ ({(got != want).sum()} incl. marginal)"
+    assert want.mean() > 0.05
 
 
 def test_bvh_counts_match_reference_traversal_order_of_magnitude(ctx, O, mesh):

@@ -1,0 +1,124 @@
+"""Served mode (continuous batching) and the autotuner, through the C ABI.
+
+Serving admits renders on the engine's own thread as request slots and the
+device-memory budget free up; a request that arrives while others are on the
+GPU shares the path queue with them.  Each result must be the same as the
+render alone (plain method): every path's random numbers are a hash of
+(seed, pixel, sample, fork, bounce) and pixels accumulate in FP64, so only
+the FP64 summation order differs (tolerance rtol 1e-6, atol 1e-7, the same
+as the batched-invariance test).
+"""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN, scene_path
+
+pytestmark = pytest.mark.gpu
+
+RTOL, ATOL = 1e-6, 1e-7
+
+
+def _requests():
+    from pcr_b200 import capi
+    rng = np.random.default_rng(77)
+    out = []
+    for k in range(14):
+        w = int(rng.choice([48, 64, 96, 128, 160]))
+        h = int(rng.choice([48, 64, 96, 128]))
+        out.append((["cornell", "cornell-glass", "cornell-spheres"][k % 3],
+                    capi.render_desc(w, h, depth=int(rng.integers(2, 7)), samples=int(rng.integers(1, 24)),
+                                     shadow=int(rng.integers(1, 5)), spectral=bool(k % 4 != 3), seed=500 + k)))
+    return out
+
+
+def test_served_results_match_alone():
+    """Requests arrive from another thread while earlier ones are in flight;
+    a small memory budget makes later ones wait for admission.  Every
+    result equals its plain render."""
+    from pcr_b200 import capi
+    reqs = _requests()
+    biggest = max(d.width * d.height for _, d in reqs) * 3 * 13
+    ctx = capi.Context(device=0, queue_capacity=1 << 17, memory_budget=3 * biggest)
+    try:
+        sids = {v: ctx.load_scene_json(scene_path(v), GOLDEN) for v in {v for v, _ in reqs}}
+        alone = [ctx.render(sids[v], d)[0] for v, d in reqs]
+        ctx.serve_start()
+        ids = [None] * len(reqs)
+
+        def producer():
+            for k, (v, d) in enumerate(reqs):
+                ids[k] = ctx.submit(sids[v], d)
+                time.sleep(0.003)
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        results, stats = [], []
+        for rid in ids:
+            ctx.wait(rid, 120_000)
+            hdr, rgb, st = ctx.fetch(rid)
+            results.append(hdr)
+            stats.append(st)
+        ctx.serve_stop()
+        for (v, d), a, m in zip(reqs, alone, results):
+            assert np.allclose(a, m, rtol=RTOL, atol=ATOL), (v, d.width, d.height)
+        # the budget held some requests back: they waited for admission
+        assert max(s.queue_ms for s in stats) > 0.0
+        assert all(s.latency_ms >= s.queue_ms for s in stats)
+        assert all(s.paths == d.width * d.height * d.samples for (_, d), s in zip(reqs, stats))
+    finally:
+        ctx.close()
+
+
+def test_cancel_pending_request():
+    """A request still waiting for admission can be cancelled; waiting on it
+    then reports PCR_ERR_CANCELLED, and the others complete unchanged."""
+    from pcr_b200 import capi
+    ctx = capi.Context(device=0, queue_capacity=1 << 17, memory_budget=256 * 256 * 3 * 13)
+    try:
+        sid = ctx.load_scene_json(scene_path("cornell"), GOLDEN)
+        d0 = capi.render_desc(256, depth=3, samples=8, shadow=2, seed=1)
+        d1 = capi.render_desc(256, depth=3, samples=8, shadow=2, seed=2)
+        ref1 = ctx.render(sid, d1)[0]
+        r0 = ctx.submit(sid, d0)
+        r1 = ctx.submit(sid, d1)
+        r2 = ctx.submit(sid, d0)   # cannot be admitted while r0 holds the whole budget
+        ctx.cancel(r2)
+        with pytest.raises(capi.PcrError) as e:
+            ctx.wait(r2, 60_000)
+        assert e.value.status == 7
+        ctx.wait(r0, 60_000)
+        ctx.wait(r1, 60_000)
+        ctx.fetch(r0, want_hdr=False, want_rgb=False)
+        assert np.allclose(ctx.fetch(r1)[0], ref1, rtol=RTOL, atol=ATOL)
+        with pytest.raises(capi.PcrError):
+            ctx.cancel(r1 + 1000)
+    finally:
+        ctx.close()
+
+
+def test_autotune_picks_from_grid_and_keeps_results():
+    """The autotuner times trial batches over queue capacity, block size,
+    issue chunk and refill cadence; the chosen tuning is one of the grid's
+    and renders are unchanged by it."""
+    from pcr_b200 import capi
+    ctx = capi.Context(device=0)
+    try:
+        sid = ctx.load_scene_json(scene_path("cornell-glass"), GOLDEN)
+        descs = [capi.render_desc(64 + 16 * k, depth=4, samples=4, shadow=2, seed=900 + k) for k in range(4)]
+        before = [ctx.render(sid, d)[0] for d in descs]
+        chosen = ctx.autotune([sid] * len(descs), descs)
+        assert chosen["queue_capacity"] in (1 << 19, 1 << 20, 1 << 21)
+        assert chosen["block_size"] in (64, 128, 256)
+        assert chosen["chunk_paths"] in (1 << 14, 1 << 16)
+        assert chosen["regen_every"] in (1, 2)
+        st = ctx.stats()
+        assert all(st[k] == chosen[k] for k in chosen)
+        ids = [ctx.submit(sid, d) for d in descs]
+        ctx.run_until_idle()
+        for b, i in zip(before, ids):
+            assert np.allclose(ctx.fetch(i)[0], b, rtol=RTOL, atol=ATOL)
+    finally:
+        ctx.close()
