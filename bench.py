@@ -69,17 +69,22 @@ def peaks():
 
 
 class Clocks:
-    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+    """nvidia-smi sampling of SM clocks and throttle reasons.  The sampler is
+    started before the warm-up (its start-up queries the driver, which must
+    not fall inside the timed region) and runs through the timed region; the
+    summary keeps the samples whose timestamps lie inside the timed window."""
 
-    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+    Q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
     def __init__(self, device: int):
         self.device = device
         self.proc = None
+        self.out = ""
+        self.win = None
 
-    def __enter__(self):
+    def start(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
                                           "-i", str(self.device), "-lms", "200"], stdout=subprocess.PIPE,
@@ -88,8 +93,9 @@ class Clocks:
             self.proc = None
         return self
 
-    def __exit__(self, *a):
-        self.out = ""
+    def stop(self, window):
+        """window: (t0, t1) of the timed region, time.time() seconds."""
+        self.win = window
         if self.proc:
             self.proc.terminate()
             try:
@@ -98,19 +104,24 @@ class Clocks:
                 self.proc.kill()
 
     def summary(self):
+        import datetime
         rows = []
         for line in (self.out or "").splitlines():
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) == 7:
+            if len(parts) == 8:
                 try:
-                    rows.append([float(parts[0]), float(parts[1]), parts[2]] + parts[3:])
+                    ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                    rows.append([ts, float(parts[1]), float(parts[2]), parts[3]] + parts[4:])
                 except ValueError:
                     pass
+        if self.win:
+            inside = [r for r in rows if self.win[0] - 0.05 <= r[0] <= self.win[1] + 0.05]
+            rows = inside or rows
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[3 + k].lower() == "active"})
-        return {"sm_mhz": float(np.median([r[0] for r in rows])), "sm_max_mhz": max(r[1] for r in rows),
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[4 + k].lower() == "active"})
+        return {"sm_mhz": float(np.median([r[1] for r in rows])), "sm_max_mhz": max(r[2] for r in rows),
                 "samples": len(rows), "reasons": reasons}
 
 
@@ -354,18 +365,21 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.SUM)
         return float(t.item())
 
+    clk = Clocks(local).start()
     for _ in range(a.warmup):
         batched_step()
     ctx.reset_stats()
     # ---- device-timed batched region
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with Clocks(local) as clk:
-        ev0.record(stream)
-        for _ in range(a.steps):
-            batched_step()
-        ev1.record(stream)
-        torch.cuda.synchronize()
+    t_w0 = time.time()
+    ev0.record(stream)
+    for _ in range(a.steps):
+        batched_step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    t_w1 = time.time()
+    clk.stop((t_w0, t_w1))
     barrier()
     ms = max_over_ranks(ev0.elapsed_time(ev1))
     st = ctx.stats()

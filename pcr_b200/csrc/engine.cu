@@ -104,7 +104,17 @@ Engine::Engine(const pcr_ctx_opts* o)
     slot_owner_.assign(kMaxActive, -1);
     scenes_.reserve(256);
     for (auto& e : prof_ev_) CK(cudaEventCreate(&e));
-    CK(cudaEventCreateWithFlags(&ev_snap_, cudaEventDisableTiming));
+    for (auto& e : ev_snaps_) CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    // Per-request buffers come from the engine's own stream-ordered pool,
+    // which keeps freed memory for reuse (release threshold: never) so that
+    // a steady request stream does no device page mapping after warm-up.
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device_;
+    CK(cudaMemPoolCreate(&pool_, &props));
+    uint64_t keep = UINT64_MAX;
+    CK(cudaMemPoolSetAttribute(pool_, cudaMemPoolAttrReleaseThreshold, &keep));
     alloc_buffers();
 }
 
@@ -118,19 +128,22 @@ Engine::~Engine()
     cudaStreamSynchronize(stream_);
     for (auto& kv : reqs_) {
         Request& r = *kv.second;
-        if (r.accum) cudaFree(r.accum);
-        if (r.d_hdr) cudaFree(r.d_hdr);
-        if (r.d_rgb) cudaFree(r.d_rgb);
+        if (r.accum) cudaFreeAsync(r.accum, stream_);
+        if (r.d_hdr) cudaFreeAsync(r.d_hdr, stream_);
+        if (r.d_rgb) cudaFreeAsync(r.d_rgb, stream_);
         if (r.ev_ready) cudaEventDestroy(r.ev_ready);
     }
+    cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(copy_stream_);
     if (staging_) cudaFreeHost(staging_);
     cudaStreamDestroy(copy_stream_);
     for (auto& s : scenes_)
         for (void* p : s.allocs) cudaFree(p);
     free_buffers();
     for (auto& e : prof_ev_) cudaEventDestroy(e);
-    cudaEventDestroy(ev_snap_);
+    for (auto& e : ev_snaps_) cudaEventDestroy(e);
     if (graph_exec_) cudaGraphExecDestroy(graph_exec_);
+    if (pool_) cudaMemPoolDestroy(pool_);
     cudaStreamDestroy(stream_);
 }
 
@@ -159,7 +172,13 @@ void Engine::alloc_buffers()
     CK(cudaMemset(d_done_, 0, 4 * kMaxActive));
     CK(cudaMemset(d_nactive_, 0, 4));
     CK(cudaMemset(d_cnt_, 0, sizeof(Counters)));
-    CK(cudaMallocHost(&h_snap_, sizeof(HostSnap)));
+    for (auto& h : h_snaps_) {
+        CK(cudaMallocHost(&h, sizeof(HostSnap)));
+        std::memset(h, 0, sizeof(HostSnap));
+    }
+    h_snap_ = h_snaps_[0];
+    snap_next_ = 0;
+    snap_inflight_ = 0;
     CK(cudaMallocHost(&h_params_, sizeof(EngineParams)));
 
     const int fill = tune_.queue_capacity;
@@ -185,7 +204,10 @@ void Engine::free_buffers()
 {
     for (void* p : qallocs_) cudaFree(p);
     qallocs_.clear();
-    if (h_snap_) cudaFreeHost(h_snap_);
+    for (auto& h : h_snaps_) {
+        if (h) cudaFreeHost(h);
+        h = nullptr;
+    }
     if (h_params_) cudaFreeHost(h_params_);
     h_snap_ = nullptr;
     h_params_ = nullptr;
@@ -614,10 +636,10 @@ void Engine::activate(Request& r, int slot)
 {
     const pcr_render_desc& d = r.desc;
     const int64_t px = (int64_t)d.width * d.height;
-    CK(cudaMallocAsync(&r.accum, px * 3 * sizeof(double), stream_));
+    CK(cudaMallocFromPoolAsync(&r.accum, px * 3 * sizeof(double), pool_, stream_));
     CK(cudaMemsetAsync(r.accum, 0, px * 3 * sizeof(double), stream_));
-    CK(cudaMallocAsync(&r.d_hdr, px * 3 * sizeof(float), stream_));
-    CK(cudaMallocAsync(&r.d_rgb, px * 3, stream_));
+    CK(cudaMallocFromPoolAsync(&r.d_hdr, px * 3 * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&r.d_rgb, px * 3, pool_, stream_));
     const SceneEntry& S = scenes_[r.scene];
     DRequest R{};
     R.scene = r.scene;
@@ -646,6 +668,7 @@ void Engine::activate(Request& r, int slot)
     k_admit<<<1, 1, 0, stream_>>>(view(), R, slot);
     CK(cudaGetLastError());
     r.slot = slot;
+    r.admit_block = blocks_launched_;
     r.state = ReqState::Active;
     r.t_admit = std::chrono::steady_clock::now();
     slot_owner_[slot] = r.id;
@@ -824,7 +847,9 @@ void Engine::harvest(bool)
     std::vector<int> keep;
     for (int s : active_slots_) {
         Request& r = *reqs_[slot_owner_[s]];
-        if (h_snap_->done[s]) {
+        // a copy taken before the slot was set for this request still
+        // holds the slot's previous owner's done flag
+        if (h_snap_->done[s] && h_snap_block_ > r.admit_block) {
             const unsigned long long tf = h_snap_->tf[s], td = h_snap_->td[s];
             r.device_ms = (td > tf && tf) ? (double)(td - tf) * 1e-6 : 0.0;
             r.paths = (uint64_t)r.desc.width * r.desc.height * r.desc.samples * std::max(1, r.desc.aa_samples);
@@ -851,6 +876,11 @@ void Engine::harvest(bool)
 }
 
 // One round of the device loop.  Returns false when nothing is left to do.
+// Launches one block of iterations and copies the device state out after it;
+// the host harvests the copies that have landed and waits only when
+// kSnapRing blocks are queued, so later blocks are queued behind the one
+// running.  A request harvested from block k's copy had no paths left, so the
+// blocks already queued behind it do no work for it.
 bool Engine::engine_step()
 {
     CK(cudaSetDevice(device_));
@@ -862,22 +892,47 @@ bool Engine::engine_step()
         for (auto& kv : reqs_)
             if (kv.second->state == ReqState::Resolving) { resolving = true; break; }
         if (active_slots_.empty()) {
-            if (resolving) {
+            if (resolving || snap_inflight_) {
                 CK(cudaStreamSynchronize(stream_));
+                if (snap_inflight_) {
+                    const int last = (snap_next_ + kSnapRing - 1) % kSnapRing;
+                    h_snap_ = h_snaps_[last];
+                    h_snap_block_ = snap_block_[last];
+                }
+                snap_inflight_ = 0;
                 harvest(true);
             }
             return !pending_.empty();
         }
     }
     launch_block();
-    CK(cudaMemcpyAsync(&h_snap_->cnt, d_cnt_, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(h_snap_->done, d_done_, sizeof(int) * kMaxActive, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(h_snap_->tf, d_tfirst_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaMemcpyAsync(h_snap_->td, d_tdone_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
-    CK(cudaEventRecord(ev_snap_, stream_));
-    CK(cudaEventSynchronize(ev_snap_));
-    std::lock_guard<std::mutex> g(mu_);
-    harvest(false);
+    blocks_launched_++;
+    const int b = snap_next_;
+    snap_block_[b] = blocks_launched_;
+    HostSnap* hs = h_snaps_[b];
+    CK(cudaMemcpyAsync(&hs->cnt, d_cnt_, sizeof(Counters), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(hs->done, d_done_, sizeof(int) * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(hs->tf, d_tfirst_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(hs->td, d_tdone_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaEventRecord(ev_snaps_[b], stream_));
+    snap_next_ = (snap_next_ + 1) % kSnapRing;
+    snap_inflight_++;
+    // harvest every copy that has landed; block only when the ring is full
+    while (snap_inflight_ > 0) {
+        const int old = (snap_next_ + kSnapRing - snap_inflight_) % kSnapRing;
+        if (snap_inflight_ < kSnapRing) {
+            const cudaError_t q = cudaEventQuery(ev_snaps_[old]);
+            if (q == cudaErrorNotReady) break;
+            CK(q);
+        } else {
+            CK(cudaEventSynchronize(ev_snaps_[old]));
+        }
+        snap_inflight_--;
+        h_snap_ = h_snaps_[old];
+        h_snap_block_ = snap_block_[old];
+        std::lock_guard<std::mutex> g(mu_);
+        harvest(false);
+    }
     return true;
 }
 
@@ -886,8 +941,10 @@ void Engine::run_until_idle()
     std::lock_guard<std::mutex> g(run_mu_);
     if (serving_) throw PcrError(PCR_ERR_INVALID, "engine is serving on its own thread");
     int64_t guard = 0;
-    uint64_t last_paths = ~0ull;
+    uint64_t last_paths = ~0ull, last_block = h_snap_block_;
     while (engine_step()) {
+        if (h_snap_block_ == last_block) continue;  // no new copy harvested
+        last_block = h_snap_block_;
         // no-progress guard: the loop must make progress every few blocks
         if (h_snap_->cnt.paths == last_paths && h_snap_->cnt.queue_n[0] == 0 && h_snap_->cnt.queue_n[1] == 0) {
             if (++guard > 64) throw PcrError(PCR_ERR_TIMEOUT, "engine made no progress");
@@ -1311,11 +1368,11 @@ void Engine::trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_
     float* d_rays = nullptr;
     int *d_mat = nullptr, *d_prim = nullptr, *d_cnt = nullptr;
     float* d_t = nullptr;
-    CK(cudaMallocAsync(&d_rays, n * 6 * sizeof(float), stream_));
-    CK(cudaMallocAsync(&d_mat, n * sizeof(int), stream_));
-    CK(cudaMallocAsync(&d_prim, n * sizeof(int), stream_));
-    CK(cudaMallocAsync(&d_t, n * sizeof(float), stream_));
-    if (counts) CK(cudaMallocAsync(&d_cnt, n * 2 * sizeof(int), stream_));
+    CK(cudaMallocFromPoolAsync(&d_rays, n * 6 * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_mat, n * sizeof(int), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_prim, n * sizeof(int), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_t, n * sizeof(float), pool_, stream_));
+    if (counts) CK(cudaMallocFromPoolAsync(&d_cnt, n * 2 * sizeof(int), pool_, stream_));
     CK(cudaMemcpyAsync(d_rays, rays, n * 6 * sizeof(float), cudaMemcpyHostToDevice, stream_));
     int grid = 0;
     grid_for((const void*)k_trace_rays, 128, 0, &grid);
@@ -1341,9 +1398,9 @@ void Engine::trace_shadow(int scene, const float* rays, const float* dist2, int6
     if (n <= 0) return;
     float *d_rays = nullptr, *d_d2 = nullptr;
     int* d_b = nullptr;
-    CK(cudaMallocAsync(&d_rays, n * 6 * sizeof(float), stream_));
-    CK(cudaMallocAsync(&d_d2, n * sizeof(float), stream_));
-    CK(cudaMallocAsync(&d_b, n * sizeof(int), stream_));
+    CK(cudaMallocFromPoolAsync(&d_rays, n * 6 * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_d2, n * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_b, n * sizeof(int), pool_, stream_));
     CK(cudaMemcpyAsync(d_rays, rays, n * 6 * sizeof(float), cudaMemcpyHostToDevice, stream_));
     CK(cudaMemcpyAsync(d_d2, dist2, n * sizeof(float), cudaMemcpyHostToDevice, stream_));
     int grid = 0;
@@ -1366,9 +1423,9 @@ void Engine::eval_stage(int what, const float* params, const float* in, int64_t 
     const int out_w = (what == 0 || what == 1) ? 1 : 3;
     const int np = what == 0 ? 4 : (what == 1 ? kSpecN : 0);
     float *d_in = nullptr, *d_out = nullptr, *d_p = nullptr;
-    CK(cudaMallocAsync(&d_in, n * in_w * sizeof(float), stream_));
-    CK(cudaMallocAsync(&d_out, n * out_w * sizeof(float), stream_));
-    CK(cudaMallocAsync(&d_p, 64 * sizeof(float), stream_));
+    CK(cudaMallocFromPoolAsync(&d_in, n * in_w * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_out, n * out_w * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_p, 64 * sizeof(float), pool_, stream_));
     CK(cudaMemcpyAsync(d_in, in, n * in_w * sizeof(float), cudaMemcpyHostToDevice, stream_));
     if (np) {
         if (!params) throw PcrError(PCR_ERR_INVALID, "stage needs parameters");

@@ -52,6 +52,7 @@ struct Request {
     std::chrono::steady_clock::time_point t_submit, t_admit, t_ready;
     double device_ms = 0;
     uint64_t paths = 0;
+    uint64_t admit_block = 0;  // blocks launched before this request's slot was (re)set
 };
 
 struct EngineTuning {
@@ -147,8 +148,20 @@ private:
     int* h_active_ = nullptr;     // pinned: [0] = n, then slots
     Counters* d_cnt_ = nullptr;
     struct HostSnap { Counters cnt; int done[kMaxActive]; unsigned long long tf[kMaxActive], td[kMaxActive]; };
-    HostSnap* h_snap_ = nullptr;  // pinned
-    cudaEvent_t ev_snap_ = nullptr;
+    // Device state copied out after each block of iterations, into a ring of
+    // pinned buffers: the host keeps up to kSnapRing blocks queued and
+    // harvests each block's copy once it has landed, so the GPU does not idle
+    // while the host harvests or is briefly descheduled.
+    static constexpr int kSnapRing = 4;
+    cudaMemPool_t pool_ = nullptr;
+    HostSnap* h_snaps_[kSnapRing] = {};
+    cudaEvent_t ev_snaps_[kSnapRing] = {};
+    HostSnap* h_snap_ = nullptr;  // the snapshot harvest reads (one of h_snaps_)
+    int snap_next_ = 0;           // buffer the next block copies into
+    int snap_inflight_ = 0;       // blocks launched whose copy is not harvested
+    uint64_t blocks_launched_ = 0;
+    uint64_t snap_block_[kSnapRing] = {};  // block count each buffer's copy follows
+    uint64_t h_snap_block_ = 0;        // the same for h_snap_
     void* d_params_ = nullptr;
     void* h_params_ = nullptr;
 

@@ -265,7 +265,10 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
 // The trace kernels are latency-bound (dependent IEEE arithmetic, scattered
 // scene loads): their register budget is capped at 64 per thread (blocks of
 // up to 256, 4 per SM) so 32 or more warps stay resident per SM.
-constexpr int kTraceMaxBlock = 256, kTraceMinBlocks = 4;
+#ifndef PCR_TRACE_MIN_BLOCKS
+#define PCR_TRACE_MIN_BLOCKS 4
+#endif
+constexpr int kTraceMaxBlock = 256, kTraceMinBlocks = PCR_TRACE_MIN_BLOCKS;
 
 // Closest hit for every queued path (trace_closest).
 __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(EngineView E, int cur)
@@ -322,7 +325,10 @@ __device__ __forceinline__ int group_append(int* counter, int count)
 }
 
 // k_shade's block shape is fixed: its register budget (launch bounds) is
-// set for 128-thread blocks, 5 per SM.
+// set for 128-thread blocks, PCR_SHADE_MIN_BLOCKS per SM.
+#ifndef PCR_SHADE_MIN_BLOCKS
+#define PCR_SHADE_MIN_BLOCKS 5
+#endif
 constexpr int kShadeBlock = 128;
 
 // Per-path shading of the hit found by k_extend (code/Renderer.cpp:656-889
@@ -340,7 +346,7 @@ constexpr int kShadeBlock = 128;
 // Per-channel values live in float4 registers (no per-thread arrays, so no
 // local memory); channels a path does not carry have zero XYZ weight, so
 // they are evaluated but contribute nothing.
-__global__ void __launch_bounds__(kShadeBlock, 5) k_shade(EngineView E, int cur, int smem_mats)
+__global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(EngineView E, int cur, int smem_mats)
 {
     extern __shared__ DMaterial s_mat[];
     const DMaterial* M = E.mats;
