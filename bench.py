@@ -39,6 +39,12 @@ sys.path.insert(0, REPO)
 METRIC = "paths/s, batched+served wavefront (64 uneven spectral renders); plain per-request alongside"
 UNIT = "paths/s"
 HBM_FALLBACK = 6650.0
+# DRAM bytes (read + write) per unit of each wavefront kernel, measured with
+# ncu (dram__bytes_read.sum + dram__bytes_write.sum over every launch of one
+# 8-render step, divided by that step's rays / shadow rays; the summary and
+# command are kept in the profiles directory).  Traffic grows in proportion to
+# the units, so a launch's traffic is this figure times its units.
+NCU_DRAM_PER_UNIT = {"extend": 48.7, "shade": 420.9, "shadow": 61.5}
 
 
 def args_():
@@ -437,8 +443,11 @@ def main():
         t_ms = ps["stage_ms"][dom]
         n_l = max(1, ps["stage_launches"][dom])
         achieved = bytes_stage[dom] / (t_ms / 1e3) / 1e9
+        units = ps["shadow_rays"] if dom == "shadow" else ps["rays"]
+        traffic = NCU_DRAM_PER_UNIT[dom] * units / n_l if dom in NCU_DRAM_PER_UNIT else None
         roofline = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                    "frac": achieved / peak, "peak_kind": kind, "traffic": None,
+                    "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
+                    "traffic_note": "ncu DRAM bytes per unit (8-render capture) x units per launch",
                     "bytes_per_launch": bytes_stage[dom] / n_l, "ms_per_launch": t_ms / n_l,
                     "stage_ms": ps["stage_ms"], "stage_share": {k: v / max(1e-9, sum(ps["stage_ms"].values()))
                                                                 for k, v in ps["stage_ms"].items()}}
@@ -479,6 +488,8 @@ def main():
                        "shadow_rays": "1..8", "spectral": "hero-4",
                        "l2": "path/shadow queues ~2 GB > 126 MB L2 (no flush needed)"},
             "rays_per_s": rays,
+            "work": {"paths": step_paths * a.steps, "rays": st["rays"], "shadow_rays": st["shadow_rays"],
+                     "iterations": st.get("iterations")},
             "plain_value": plain, "batched_over_plain": (value / plain) if plain else None,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
