@@ -1376,8 +1376,10 @@ void Engine::trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_
     CK(cudaMemcpyAsync(d_rays, rays, n * 6 * sizeof(float), cudaMemcpyHostToDevice, stream_));
     int grid = 0;
     grid_for((const void*)k_trace_rays, 128, 0, &grid);
+    if (profile_) CK(cudaEventRecord(prof_ev_[0], stream_));
     k_trace_rays<<<grid, 128, 0, stream_>>>(d_scenes_ + scene, d_mats_, d_rays, n, d_mat, d_prim, d_t, bvh_only, d_cnt);
     CK(cudaGetLastError());
+    if (profile_) record_other(prof_ev_[0], prof_ev_[1]);
     if (mat) CK(cudaMemcpyAsync(mat, d_mat, n * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     if (prim) CK(cudaMemcpyAsync(prim, d_prim, n * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     if (t) CK(cudaMemcpyAsync(t, d_t, n * sizeof(float), cudaMemcpyDeviceToHost, stream_));
@@ -1388,6 +1390,17 @@ void Engine::trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_
     CK(cudaFreeAsync(d_t, stream_));
     if (d_cnt) CK(cudaFreeAsync(d_cnt, stream_));
     CK(cudaStreamSynchronize(stream_));
+}
+
+// Profiled contexts time the parity-query kernels too, under stage "other".
+void Engine::record_other(cudaEvent_t a, cudaEvent_t z)
+{
+    CK(cudaEventRecord(z, stream_));
+    CK(cudaEventSynchronize(z));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, z));
+    stage_ms_[7] += ms;
+    stage_launches_[7]++;
 }
 
 void Engine::trace_shadow(int scene, const float* rays, const float* dist2, int64_t n, int32_t* blocked)
@@ -1405,8 +1418,10 @@ void Engine::trace_shadow(int scene, const float* rays, const float* dist2, int6
     CK(cudaMemcpyAsync(d_d2, dist2, n * sizeof(float), cudaMemcpyHostToDevice, stream_));
     int grid = 0;
     grid_for((const void*)k_trace_shadow, 128, 0, &grid);
+    if (profile_) CK(cudaEventRecord(prof_ev_[0], stream_));
     k_trace_shadow<<<grid, 128, 0, stream_>>>(d_scenes_ + scene, d_mats_, d_rays, d_d2, n, d_b);
     CK(cudaGetLastError());
+    if (profile_) record_other(prof_ev_[0], prof_ev_[1]);
     CK(cudaMemcpyAsync(blocked, d_b, n * sizeof(int), cudaMemcpyDeviceToHost, stream_));
     CK(cudaFreeAsync(d_rays, stream_));
     CK(cudaFreeAsync(d_d2, stream_));

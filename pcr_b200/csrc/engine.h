@@ -87,6 +87,7 @@ public:
 
     void trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_t* prim, float* t, int bvh_only,
                int32_t* counts);
+    void record_other(cudaEvent_t a, cudaEvent_t z);
     void trace_shadow(int scene, const float* rays, const float* dist2, int64_t n, int32_t* blocked);
     void eval_stage(int what, const float* params, const float* in, int64_t n, float* out);
 

@@ -257,7 +257,7 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
         Q.o[pos] = make_float4(R.cam_x, R.cam_y, R.cam_z, lambda0);
         Q.d[pos] = make_float4(d.x, d.y, d.z, __int_as_float(nch << 12));
         Q.tp[pos] = make_float4(1.f, 1.f, 1.f, 1.f);
-        Q.id[pos] = make_int4(slot, (int)pixel, (int)sample, 0);
+        Q.id[pos] = make_int4(slot, (int)pixel, (int)sample, R.scene);
     }
 }
 
@@ -278,8 +278,7 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(Engi
     const PathQueue Q = E.q[cur];
     unsigned long long mine = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int slot = Q.id[i].x;
-        const DScene& S = E.scenes[E.reqs[slot].scene];
+        const DScene& S = E.scenes[Q.id[i].w];
         float4 o = Q.o[i], d = Q.d[i];
         float t = FLT_MAX, u = 0.f, v = 0.f;
         uint32_t prim = scene_closest(S, xyz(o), xyz(d), FLT_MAX, t, u, v);
@@ -389,7 +388,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
 
         if (live && (prim & kPrimKindMask) != kPrimNone) {
             const DRequest& R = E.reqs[slot];
-            const DScene& S = E.scenes[R.scene];
+            const DScene& S = E.scenes[id.w];
             const bool spectral = (R.flags & kReqSpectral) != 0;
             spec_path = spectral;
             // wavelengths carried by this path (code/Renderer.cpp:227-239)
@@ -606,7 +605,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         const float f = G * w;
                         SQ.o[pos] = make_float4(so.x, so.y, so.z, d2);
                         SQ.d[pos] = make_float4(wi.x, wi.y, wi.z, __int_as_float(id.y));
-                        SQ.c[pos] = make_float4(V.x * f, V.y * f, V.z * f, __int_as_float(slot));
+                        SQ.c[pos] = make_float4(V.x * f, V.y * f, V.z * f, __int_as_float(slot | (id.w << 16)));
                     }
                 }
                 const float4 r0 = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 0u);
@@ -679,15 +678,14 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_shadow(Engi
         const float4 o = SQ.o[i];
         if (!(o.w >= 0.f)) continue;  // skip record (zero geometry term)
         const float4 d = SQ.d[i], c = SQ.c[i];
-        const int slot = __float_as_int(c.w);
-        const DRequest& R = E.reqs[slot];
-        const DScene& S = E.scenes[R.scene];
+        const int tag = __float_as_int(c.w);
+        const DScene& S = E.scenes[tag >> 16];
         const float d2 = o.w;
         // a hit beyond the light cannot block: bound the query just past it
         const float tmax = sqrtf(d2) * 1.0001f + 1e-4f;
         mine++;
         if (!scene_blocked(S, E.mats, xyz(o), xyz(d), tmax, (double)d2 - 1e-3))
-            add_xyz(R.accum + (size_t)__float_as_int(d.w) * 3, make_float3(c.x, c.y, c.z));
+            add_xyz(E.reqs[tag & 0xFFFF].accum + (size_t)__float_as_int(d.w) * 3, make_float3(c.x, c.y, c.z));
     }
     for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, off);
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&C->shadow_rays, mine);

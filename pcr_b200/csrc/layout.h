@@ -122,7 +122,7 @@ struct PathQueue {
     float4* o;     // origin, hero lambda
     float4* d;     // direction, meta (bits): bounce | fork<<8 | single<<11 | n<<12
     float4* tp;    // throughput per channel
-    int4* id;      // request slot, pixel, sample, unused
+    int4* id;      // request slot, pixel, sample, scene (copied by continuations and forks)
     // XYZ weight of each carried wavelength, cmf(lambda_k) * 300/yBarIntegral / N
     // (spectral paths only): w[0] = x0 y0 z0 x1, w[1] = y1 z1 x2 y2, w[2] = z2 x3 y3 z3.
     // Computed once at raygen; a path's wavelengths never change.
@@ -132,7 +132,7 @@ struct PathQueue {
 struct ShadowQueue {
     float4* o;     // origin, lightDist2
     float4* d;     // direction, pixel (bits)
-    float4* c;     // contribution (XYZ or RGB), request slot (bits)
+    float4* c;     // contribution (XYZ or RGB), request slot | scene << 16 (bits)
 };
 
 struct Counters {
