@@ -134,35 +134,6 @@ __device__ __forceinline__ bool tri_hit(float4 a, float4 b, float4 c, float3 o, 
     return true;
 }
 
-// Slab test of one child box with the reference's arithmetic
-// (code/Bvh/Bvh.cpp:360-377); inv = 1/dir per axis, NaN lanes ignored the
-// way std::max/std::min ignore a NaN second argument.
-__device__ __forceinline__ bool slab(float lx, float hx, float ly, float hy, float lz, float hz, float3 o, float3 inv,
-                                     float segMax, float& tNear)
-{
-    using namespace ex;
-    float tmin = 0.f, tmax = segMax;
-    float t1 = mul(sub(lx, o.x), inv.x), t2 = mul(sub(hx, o.x), inv.x);
-    if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
-    tmin = (tmin < t1) ? t1 : tmin;
-    tmax = (t2 < tmax) ? t2 : tmax;
-    if (tmin > tmax) return false;
-    t1 = mul(sub(ly, o.y), inv.y); t2 = mul(sub(hy, o.y), inv.y);
-    if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
-    tmin = (tmin < t1) ? t1 : tmin;
-    tmax = (t2 < tmax) ? t2 : tmax;
-    if (tmin > tmax) return false;
-    t1 = mul(sub(lz, o.z), inv.z); t2 = mul(sub(hz, o.z), inv.z);
-    if (t1 > t2) { float s = t1; t1 = t2; t2 = s; }
-    tmin = (tmin < t1) ? t1 : tmin;
-    tmax = (t2 < tmax) ? t2 : tmax;
-    if (tmin > tmax) return false;
-    tNear = tmin;
-    return true;
-}
-
-struct TraceCounts { int nodes, tris; };
-
 // The shadow test's distance check (code/Renderer.cpp:852-860): a hit at t
 // blocks when lightDist2 - 1e-3 > |hit - origin|^2, the hit point and its
 // squared distance taken with the reference's float operations and the
@@ -175,67 +146,115 @@ __device__ __forceinline__ bool blocks_at(float3 o, float3 d, float t, double li
     return lim > (double)ex::dot(dd, dd);
 }
 
-// Closest hit over the 4-wide BVH (ordered traversal, stack in local memory).
-// `closest` comes in as the best t from spheres/planes.  Returns the leaf-order
-// triangle index or -1; t/u/v of the hit.  With kAny (shadow rays over a
-// mesh without emissive triangles) it returns -2 as soon as a hit closer
-// than `closest` blocks (blocks_at with `lim`).
+// One child box of a 4-wide node with the reference's slab arithmetic
+// (code/Bvh/Bvh.cpp:360-377), branch-free: the reference returns at the
+// first axis where tmin > tmax, and since tmin only grows and tmax only
+// shrinks, testing once after all three axes gives the same answer.  NaN
+// lanes are ignored the way std::max/std::min ignore a NaN second argument.
+// Returns tNear, or +inf for a miss.
+__device__ __forceinline__ float slab4(float lx, float hx, float ly, float hy, float lz, float hz, float3 o, float3 inv,
+                                       float segMax)
+{
+    using namespace ex;
+    float tmin = 0.f, tmax = segMax;
+    float t1 = mul(sub(lx, o.x), inv.x), t2 = mul(sub(hx, o.x), inv.x);
+    float a = t1 > t2 ? t2 : t1, b = t1 > t2 ? t1 : t2;
+    tmin = (tmin < a) ? a : tmin;
+    tmax = (b < tmax) ? b : tmax;
+    t1 = mul(sub(ly, o.y), inv.y); t2 = mul(sub(hy, o.y), inv.y);
+    a = t1 > t2 ? t2 : t1; b = t1 > t2 ? t1 : t2;
+    tmin = (tmin < a) ? a : tmin;
+    tmax = (b < tmax) ? b : tmax;
+    t1 = mul(sub(lz, o.z), inv.z); t2 = mul(sub(hz, o.z), inv.z);
+    a = t1 > t2 ? t2 : t1; b = t1 > t2 ? t1 : t2;
+    tmin = (tmin < a) ? a : tmin;
+    tmax = (b < tmax) ? b : tmax;
+    return tmin > tmax ? __int_as_float(0x7f800000) : tmin;
+}
+
+__device__ __forceinline__ void cas(float& ta, int& ca, float& tb, int& cb)
+{
+    if (tb < ta) {
+        const float t = ta; ta = tb; tb = t;
+        const int c = ca; ca = cb; cb = c;
+    }
+}
+
+struct TraceCounts { int nodes, tris; };
+
+// Closest hit over the 4-wide BVH: ordered traversal with the stack in
+// local memory; the nearest hit child is visited next without a push, the
+// others are pushed far-to-near.  `closest` comes in as the best t from
+// spheres/planes.  Returns the leaf-order triangle index or -1; t/u/v of the
+// hit.  With kAny (shadow rays over a mesh without emissive triangles) it
+// returns -2 as soon as a hit closer than `closest` blocks (blocks_at with
+// `lim`).  Empty child slots carry the code 0x80000000 (a leaf of no
+// triangles).
 template <bool kCount, bool kAny = false>
 __device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d, float& closest, float& hu, float& hv,
                                             TraceCounts* cnt, double lim = 0.0)
 {
     if (S.n_nodes <= 0) return -1;
-    float3 inv = make_float3(__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdiv_rn(1.f, d.z));
+    const float inf = __int_as_float(0x7f800000);
+    const float3 inv = make_float3(__fdiv_rn(1.f, d.x), __fdiv_rn(1.f, d.y), __fdiv_rn(1.f, d.z));
     int stk[kStackSize];
     float stt[kStackSize];
     int top = 0;
     int best = -1;
-    stk[top] = 0; stt[top] = 0.f; top++;
-    while (top > 0) {
-        --top;
-        int code = stk[top];
-        if (stt[top] > closest) continue;
-        if (code >= 0) {
-            const DNode4* n = S.nodes + code;
-            float4 lx = __ldg(&n->lox), hx = __ldg(&n->hix), ly = __ldg(&n->loy), hy = __ldg(&n->hiy);
-            float4 lz = __ldg(&n->loz), hz = __ldg(&n->hiz);
-            int4 ch = __ldg(&n->child), va = __ldg(&n->valid);
-            if (kCount) cnt->nodes++;
-            float tn[4];
-            int cc[4];
-            int k = 0;
-            float t;
-            if (va.x && slab(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.x; k++; }
-            if (va.y && slab(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.y; k++; }
-            if (va.z && slab(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.z; k++; }
-            if (va.w && slab(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, o, inv, closest, t)) { tn[k] = t; cc[k] = ch.w; k++; }
-            // push far-to-near so the nearest child pops first
-            for (int i = 1; i < k; i++) {
-                float kt = tn[i];
-                int kc = cc[i];
-                int j = i - 1;
-                while (j >= 0 && tn[j] < kt) { tn[j + 1] = tn[j]; cc[j + 1] = cc[j]; j--; }
-                tn[j + 1] = kt; cc[j + 1] = kc;
-            }
-            if (top + k > kStackSize) continue;  // mirrors the reference's overflow guard
-            for (int i = 0; i < k; i++) { stk[top] = cc[i]; stt[top] = tn[i]; top++; }
-        } else {
-            int first = code & 0x00FFFFFF;
-            int count = (code >> 24) & 0x7F;
-            for (int i = 0; i < count; i++) {
-                const DTri* tr = S.tris + first + i;
-                float4 a = __ldg(&tr->v0_id), b = __ldg(&tr->e1_mat), c = __ldg(&tr->e2_flags);
-                if (kCount) cnt->tris++;
-                float t, u, v;
-                if (tri_hit(a, b, c, o, d, closest, t, u, v)) {
-                    if (kAny && blocks_at(o, d, t, lim)) return -2;
-                    closest = t;
-                    hu = u;
-                    hv = v;
-                    best = first + i;
+    int code = 0;        // the root
+    float tcode = 0.f;
+    while (true) {
+        if (!(tcode > closest)) {
+            if (code >= 0) {
+                const DNode4* n = S.nodes + code;
+                const float4 lx = __ldg(&n->lox), hx = __ldg(&n->hix), ly = __ldg(&n->loy), hy = __ldg(&n->hiy);
+                const float4 lz = __ldg(&n->loz), hz = __ldg(&n->hiz);
+                const int4 ch = __ldg(&n->child);
+                if (kCount) cnt->nodes++;
+                const int kEmpty = (int)0x80000000u;
+                float t0 = ch.x != kEmpty ? slab4(lx.x, hx.x, ly.x, hy.x, lz.x, hz.x, o, inv, closest) : inf;
+                float t1 = ch.y != kEmpty ? slab4(lx.y, hx.y, ly.y, hy.y, lz.y, hz.y, o, inv, closest) : inf;
+                float t2 = ch.z != kEmpty ? slab4(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, o, inv, closest) : inf;
+                float t3 = ch.w != kEmpty ? slab4(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, o, inv, closest) : inf;
+                int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
+                // ascending by tNear; misses (+inf) last
+                cas(t0, c0, t1, c1);
+                cas(t2, c2, t3, c3);
+                cas(t0, c0, t2, c2);
+                cas(t1, c1, t3, c3);
+                cas(t1, c1, t2, c2);
+                const int k = (t0 < inf) + (t1 < inf) + (t2 < inf) + (t3 < inf);
+                // the reference skips all children when they would overflow its stack
+                if (k > 0 && top + k - 1 <= kStackSize) {
+                    if (k > 3) { stk[top] = c3; stt[top] = t3; top++; }
+                    if (k > 2) { stk[top] = c2; stt[top] = t2; top++; }
+                    if (k > 1) { stk[top] = c1; stt[top] = t1; top++; }
+                    code = c0;
+                    tcode = t0;
+                    continue;
+                }
+            } else {
+                const int first = code & 0x00FFFFFF;
+                const int count = (code >> 24) & 0x7F;
+                for (int i = 0; i < count; i++) {
+                    const DTri* tr = S.tris + first + i;
+                    float4 a = __ldg(&tr->v0_id), b = __ldg(&tr->e1_mat), c = __ldg(&tr->e2_flags);
+                    if (kCount) cnt->tris++;
+                    float t, u, v;
+                    if (tri_hit(a, b, c, o, d, closest, t, u, v)) {
+                        if (kAny && blocks_at(o, d, t, lim)) return -2;
+                        closest = t;
+                        hu = u;
+                        hv = v;
+                        best = first + i;
+                    }
                 }
             }
         }
+        if (top == 0) break;
+        --top;
+        code = stk[top];
+        tcode = stt[top];
     }
     return best;
 }

@@ -538,6 +538,20 @@ int Engine::upload_scene(const pcr_scene_desc& d)
     S.sgroups = dupload(sgroups, e.allocs, bytes);
     S.n_sgroups = (int)sgroups.size() / 2;
     S.emissive_tris = emissive_tris;
+    {
+        int only = -1, n_emit = 0;
+        for (int i = 0; i < d.n_materials; i++)
+            if (e.mats[i].flags & kMatEmissive) { only = i; n_emit++; }
+        bool all_lights = n_emit == 1;
+        for (int i = 0; i < d.n_lights && all_lights; i++) {
+            const pcr_light& L = d.lights[i];
+            if (L.kind == 0) all_lights = L.plane.mat == only;
+            else
+                for (int k = L.tri_offset; k < L.tri_offset + L.tri_count; k++)
+                    if (d.light_triangles[k].mat != only) all_lights = false;
+        }
+        S.emit_mat = all_lights ? only : -1;
+    }
     S.n_emit_spheres = S.n_emit_planes = 0;
     for (int i = 0; i < d.n_spheres; i++)
         if (spheres[i].mat.y) {

@@ -252,7 +252,17 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
                 if (l > 700.f) l -= span;
                 lam[k] = k < nch ? l : lam[0];
             }
-            store_weights(Q, pos, xyz_weights(true, lam, nch, 1.f / (float)nch, xyz_scale));
+            XyzWeights W = xyz_weights(true, lam, nch, 1.f / (float)nch, xyz_scale);
+            const DScene& S = E.scenes[R.scene];
+            if (S.emit_mat >= 0) {
+                // emission of the scene's only emissive material, folded in
+                const float4 e = spec4(E.mats[S.mat_base + S.emit_mat], 1, make_float4(lam[0], lam[1], lam[2], lam[3]));
+                W.w[0] = f3mul(W.w[0], e.x);
+                W.w[1] = f3mul(W.w[1], e.y);
+                W.w[2] = f3mul(W.w[2], e.z);
+                W.w[3] = f3mul(W.w[3], e.w);
+            }
+            store_weights(Q, pos, W);
         }
         Q.o[pos] = make_float4(R.cam_x, R.cam_y, R.cam_z, lambda0);
         Q.d[pos] = make_float4(d.x, d.y, d.z, __int_as_float(nch << 12));
@@ -440,7 +450,9 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
             const DMaterial& m = M[S.mat_base + mi];
             const bool last = bounce + 1 >= R.depth;
             if (m.flags & kMatEmissive) {
-                const float4 c = mul4(tp4, spectral ? spec4(m, 1, lam4) : rgb4(m.emissive));
+                // with emit_mat the carried weights already hold the emission
+                const float4 c = !spectral ? mul4(tp4, rgb4(m.emissive))
+                               : S.emit_mat >= 0 ? tp4 : mul4(tp4, spec4(m, 1, lam4));
                 const XyzWeights W = spectral ? load_weights(Q, i) : rgb_weights();
                 emit_xyz = apply_xyz(W, c);
                 emit = true;
@@ -593,7 +605,8 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         if (lm != cached) {
                             // spectral product of this light material, once per vertex
                             const DMaterial& lmat = M[S.mat_base + lm];
-                            const float4 c = mul4(tpal, spectral ? spec4(lmat, 1, lam4) : rgb4(lmat.emissive));
+                            const float4 c = !spectral ? mul4(tpal, rgb4(lmat.emissive))
+                                           : S.emit_mat >= 0 ? tpal : mul4(tpal, spec4(lmat, 1, lam4));
                             V = f3mul(apply_xyz(W, c), scaleS);
                             cached = lm;
                         }

@@ -64,7 +64,7 @@ struct alignas(16) DTri {
 // boxes are the binary nodes' boxes verbatim.  8 x 16 B = 128 B.
 struct alignas(16) DNode4 {
     float4 lox, hix, loy, hiy, loz, hiz;
-    int4 child;   // >= 0: internal node index; leaf: 0x80000000 | count<<24 | first
+    int4 child;   // >= 0: internal node index; leaf: 0x80000000 | count<<24 | first; empty slot: 0x80000000
     int4 valid;   // 1 for a used slot, 0 for empty
 };
 
@@ -97,6 +97,11 @@ struct DScene {
     int n_planes, n_spheres, n_nodes, n_tris, n_lights, mat_base, n_mats, n_pgroups;
     int n_sgroups;
     int emissive_tris;        // 1 when any triangle's material is emissive
+    // The scene's only emissive material (scene-local index) when it has
+    // exactly one and every light uses it, else -1.  Spectral paths of such
+    // a scene carry emission x XYZ weight per wavelength instead of the
+    // weight alone.
+    int emit_mat;
     // Emissive spheres and planes (indices), for the shadow query's first
     // pass; n_emit_* = -1 when a scene has more than kMaxEmitPrims of a kind.
     int n_emit_spheres, n_emit_planes;
@@ -125,7 +130,9 @@ struct PathQueue {
     int4* id;      // request slot, pixel, sample, scene (copied by continuations and forks)
     // XYZ weight of each carried wavelength, cmf(lambda_k) * 300/yBarIntegral / N
     // (spectral paths only): w[0] = x0 y0 z0 x1, w[1] = y1 z1 x2 y2, w[2] = z2 x3 y3 z3.
-    // Computed once at raygen; a path's wavelengths never change.
+    // Computed once at raygen; a path's wavelengths never change.  In a scene
+    // with one emissive material (DScene::emit_mat >= 0) each weight is
+    // multiplied by that material's emission at the wavelength.
     float4* w[3];
 };
 

@@ -666,7 +666,9 @@ std::vector<DNode4> collapse_bvh4(const std::vector<pcr_bvh_node>& bvh, int n_tr
             ch.insert(ch.begin() + pick, {bvh[c].left_or_first, bvh[c].right_child});
         }
         float lo[3][4], hi[3][4];
-        int code[4] = {0, 0, 0, 0}, valid[4] = {0, 0, 0, 0};
+        // empty slots: the code of a leaf with no triangles
+        const int empty = (int)0x80000000u;
+        int code[4] = {empty, empty, empty, empty}, valid[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; k++)
             for (int a = 0; a < 3; a++) { lo[a][k] = 0.f; hi[a][k] = 0.f; }
         for (size_t k = 0; k < ch.size(); k++) {
