@@ -543,12 +543,20 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                 const float3 h1 = hc;
                 if (S.total_light_area > 0.f) {
                     const float scaleS = S.total_light_area * inv_pi / (float)R.shadow;
-                    const XyzWeights W = spectral ? load_weights(Q, i) : rgb_weights();
                     const float4 tpal = mul4(tp4, al);
                     int cached = -1;
                     float3 V = make_float3(0.f, 0.f, 0.f);
-                    int spos = group_append(&C->shadow_n, R.shadow);
-                    for (int s = 0; s < R.shadow; s++) {
+                    if (spectral && S.emit_mat >= 0) {
+                        // every light has the one emissive material, whose
+                        // emission the carried weights already hold: the
+                        // vertex's product is known before any sample
+                        V = f3mul(apply_xyz(load_weights(Q, i), tpal), scaleS);
+                        cached = S.emit_mat;
+                    }
+                    const int spos = group_append(&C->shadow_n, R.shadow);
+                    const int nsh = spos + R.shadow <= E.shadow_cap ? R.shadow : 0;
+                    if (nsh == 0) atomicOr(&C->status, 1);
+                    for (int s = 0; s < nsh; s++) {
                         const float4 rr = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce,
                                                 1u + (uint32_t)s);
                         int pick = 0;
@@ -587,7 +595,8 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         }
                         const float3 Li = f3sub(P, hc);
                         const float d2 = f3dot(Li, Li);
-                        const float3 wi = f3mul(Li, rsqrtf(d2));
+                        const float inv_d = rsqrtf(d2);
+                        const float3 wi = f3mul(Li, inv_d);
                         const float cosT = fmaxf(0.f, f3dot(wi, N));
                         float3 so;
                         // the lit-facing branch moves the shading point again
@@ -595,19 +604,17 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         if (cosT <= 0.f) so = f3sub(hc, f3mul(N, 1e-3f));
                         else { hc = f3add(hc, f3mul(N, 1e-3f)); so = hc; }
                         const float cosL = fmaxf(0.f, -f3dot(Nl, Li));
-                        const float G = (cosT * cosL) / d2;
+                        const float G = cosT * cosL * (inv_d * inv_d);
                         const int pos = spos + s;
-                        if (pos >= E.shadow_cap) { atomicOr(&C->status, 1); continue; }
                         if (!(G > 0.f)) {
                             SQ.o[pos] = make_float4(0.f, 0.f, 0.f, -1.f);  // skip record
                             continue;
                         }
                         if (lm != cached) {
-                            // spectral product of this light material, once per vertex
+                            // product of this light material, once per vertex
                             const DMaterial& lmat = M[S.mat_base + lm];
-                            const float4 c = !spectral ? mul4(tpal, rgb4(lmat.emissive))
-                                           : S.emit_mat >= 0 ? tpal : mul4(tpal, spec4(lmat, 1, lam4));
-                            V = f3mul(apply_xyz(W, c), scaleS);
+                            const float4 c = spectral ? mul4(tpal, spec4(lmat, 1, lam4)) : mul4(tpal, rgb4(lmat.emissive));
+                            V = f3mul(apply_xyz(spectral ? load_weights(Q, i) : rgb_weights(), c), scaleS);
                             cached = lm;
                         }
                         float w = 1.f;
