@@ -271,6 +271,13 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
     }
 }
 
+// Brings the next grid-stride record's line into L2 while this one is
+// processed (no register cost; the record is read again when its turn comes).
+__device__ __forceinline__ void prefetch_l2(const void* p)
+{
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
+}
+
 // ------------------------------------------------------------------ extend
 // The trace kernels are latency-bound (dependent IEEE arithmetic, scattered
 // scene loads): their register budget is capped at 64 per thread (blocks of
@@ -288,6 +295,8 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(Engi
     const PathQueue Q = E.q[cur];
     unsigned long long mine = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int nx = i + gridDim.x * blockDim.x;
+        if (nx < n) { prefetch_l2(Q.o + nx); prefetch_l2(Q.d + nx); prefetch_l2(Q.id + nx); }
         const DScene& S = E.scenes[Q.id[i].w];
         float4 o = Q.o[i], d = Q.d[i];
         float t = FLT_MAX, u = 0.f, v = 0.f;
@@ -300,6 +309,7 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(Engi
 }
 
 // ------------------------------------------------------------------ helpers
+
 __device__ __forceinline__ int warp_append(int* counter, bool want)
 {
     const unsigned mask = __ballot_sync(0xffffffffu, want);
@@ -382,6 +392,11 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
         const bool live = i < n;
         int4 id = make_int4(0, 0, 0, 0);
         float4 o4 = make_float4(0, 0, 0, 0), d4 = o4, tp4 = o4, h = o4;
+        if (i + stride < n) {
+            const int nx = i + stride;
+            prefetch_l2(Q.id + nx); prefetch_l2(Q.o + nx); prefetch_l2(Q.d + nx); prefetch_l2(Q.tp + nx);
+            prefetch_l2(E.hit + nx);
+        }
         if (live) { id = Q.id[i]; o4 = Q.o[i]; d4 = Q.d[i]; tp4 = Q.tp[i]; h = E.hit[i]; }
         const int slot = id.x;
         const uint32_t prim = __float_as_uint(h.y);
@@ -695,6 +710,8 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_shadow(Engi
     const ShadowQueue SQ = E.sq;
     unsigned long long mine = 0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int nx = i + gridDim.x * blockDim.x;
+        if (nx < n) { prefetch_l2(SQ.o + nx); prefetch_l2(SQ.d + nx); prefetch_l2(SQ.c + nx); }
         const float4 o = SQ.o[i];
         if (!(o.w >= 0.f)) continue;  // skip record (zero geometry term)
         const float4 d = SQ.d[i], c = SQ.c[i];
