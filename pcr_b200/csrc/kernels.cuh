@@ -384,8 +384,10 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
     const ShadowQueue SQ = E.sq;
     const float inv_pi = 1.f / 3.14159274f;
     const int lane = threadIdx.x & 31;
-    // warp-uniform trip count: every lane of a warp runs the same iterations,
-    // so the warp-wide appends at the bottom see all 32 lanes
+    // block-uniform trip count: every thread of a block runs the same
+    // iterations, so the block-wide append at the bottom sees all of them
+    __shared__ int s_app[2][kShadeBlock / 32 + 1];
+    int parity = 0;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
         const int i = base + threadIdx.x;
@@ -669,11 +671,26 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
             }
         }
 
-        // ---- emit work (warp-uniform control flow from here)
+        // ---- emit work (block-uniform control flow from here)
         if (emit) add_xyz(acc, emit_xyz);
         {
             const int newMeta = (bounce + 1) | (fork << 8) | (single << 11) | (nHero << 12);
-            int pos = warp_append(&C->queue_n[cur ^ 1], cont);
+            // one contiguous range per block (its warps in order), so the
+            // next launch's warps rarely straddle two blocks' outputs, which
+            // may belong to different scenes
+            int* sw = s_app[parity];
+            parity ^= 1;
+            const unsigned am = __ballot_sync(0xffffffffu, cont);
+            const int wid = threadIdx.x >> 5;
+            if (lane == 0) sw[wid] = __popc(am);
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int tot = 0;
+                for (int k = 0; k < kShadeBlock / 32; k++) { const int c = sw[k]; sw[k] = tot; tot += c; }
+                sw[kShadeBlock / 32] = tot ? atomicAdd(&C->queue_n[cur ^ 1], tot) : 0;
+            }
+            __syncthreads();
+            int pos = cont ? sw[kShadeBlock / 32] + sw[wid] + __popc(am & ((1u << lane) - 1u)) : -1;
             if (pos >= E.queue_cap) { atomicOr(&C->status, 2); pos = -1; }
             if (pos >= 0) {
                 NQ.o[pos] = make_float4(no.x, no.y, no.z, o4.w);
