@@ -85,6 +85,12 @@ typedef struct {
 typedef struct {
     int32_t width, height, depth, samples, shadow_samples;
     int32_t spectral, hero_samples, mis, russian, stratified;
+    /* aa_samples: jittered camera rounds per pixel, each of `samples` paths.
+     * adaptive (with aa_samples > 1): a pixel stops after 4 or more rounds
+     * once every channel's relative variance of the round means is below
+     * 0.05 (code/Gpu/Opengl/OpenglRenderer.cpp:1288-1383).  denoise: two
+     * 5x5 bilateral passes on the 8-bit image, on the device
+     * (code/Denoise.cpp:14-86). */
     int32_t aa_samples, adaptive, aces, denoise;
     uint64_t seed;           /* 0 -> 1 */
     int32_t priority;        /* serving: lower runs first among equals (0 default) */

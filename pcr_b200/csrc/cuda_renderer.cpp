@@ -14,54 +14,6 @@
 
 namespace pcr {
 
-// ------------------------------------------------------------------ bilateral
-void bilateral_rgb(std::vector<uint8_t>& rgb, int width, int height)
-{
-    // 5x5 cross-bilateral, two passes (code/Denoise.cpp:14-86)
-    if (width <= 0 || height <= 0 || rgb.size() < (size_t)width * height * 3) return;
-    const int radius = 2;
-    const float invSpatial2 = 1.0f / (2.0f * 1.5f * 1.5f);
-    const float invColor2 = 1.0f / (2.0f * 10.0f * 10.0f);
-    std::vector<uint8_t> out(rgb.size());
-    for (int pass = 0; pass < 2; pass++) {
-        const std::vector<uint8_t>& src = pass == 0 ? rgb : out;
-        std::vector<uint8_t>& dst = pass == 0 ? out : rgb;
-        for (int y = 0; y < height; y++)
-            for (int x = 0; x < width; x++) {
-                const size_t c = ((size_t)y * width + x) * 3;
-                const float cR = src[c], cG = src[c + 1], cB = src[c + 2];
-                float sw = 0.f, sr = 0.f, sg = 0.f, sb = 0.f;
-                for (int dy = -radius; dy <= radius; dy++) {
-                    const int ny = y + dy;
-                    if (ny < 0 || ny >= height) continue;
-                    for (int dx = -radius; dx <= radius; dx++) {
-                        const int nx = x + dx;
-                        if (nx < 0 || nx >= width) continue;
-                        const size_t n = ((size_t)ny * width + nx) * 3;
-                        const float nR = src[n], nG = src[n + 1], nB = src[n + 2];
-                        const float sp = (float)(dx * dx + dy * dy) * invSpatial2;
-                        const float dR = nR - cR, dG = nG - cG, dB = nB - cB;
-                        const float col = (dR * dR + dG * dG + dB * dB) * invColor2;
-                        const float w = std::exp(-(sp + col));
-                        sw += w;
-                        sr += w * nR;
-                        sg += w * nG;
-                        sb += w * nB;
-                    }
-                }
-                if (sw > 0.0f) {
-                    dst[c] = (uint8_t)std::min(255.0f, sr / sw + 0.5f);
-                    dst[c + 1] = (uint8_t)std::min(255.0f, sg / sw + 0.5f);
-                    dst[c + 2] = (uint8_t)std::min(255.0f, sb / sw + 0.5f);
-                } else {
-                    dst[c] = src[c];
-                    dst[c + 1] = src[c + 1];
-                    dst[c + 2] = src[c + 2];
-                }
-            }
-    }
-}
-
 // ------------------------------------------------------------------ PNG
 namespace {
 void put32(std::vector<uint8_t>& o, uint32_t v)
@@ -199,8 +151,6 @@ bool CudaRenderer::render_to(const pcr_scene_desc& scene, RenderOutput& out)
         }
         _scene_key = key;
     }
-    if (useAdaptive)
-        std::cerr << "warning: --adaptive is not applied by the CUDA backend; rendering all aa samples.\n";
     pcr_render_desc d = desc();
     out.hdr.assign((size_t)_width * _height * 3, 0.f);
     out.rgb8.assign((size_t)_width * _height * 3, 0);
@@ -211,7 +161,7 @@ bool CudaRenderer::render_to(const pcr_scene_desc& scene, RenderOutput& out)
     }
     if (useOIDN)
         std::cerr << "warning: --oidn requested but binary was not built with PCR_USE_OIDN=ON; skipping denoise.\n";
-    if (useDenoise) bilateral_rgb(out.rgb8, _width, _height);
+    // the bilateral denoise (useDenoise) runs on the device after the resolve
     if (progressRows) progressRows->store(_height, std::memory_order_relaxed);
     if (onPartialFrame) {
         std::vector<std::array<float, 3>> fb((size_t)_width * _height);

@@ -29,9 +29,6 @@ struct RenderOutput {
     std::vector<uint8_t> rgb8;    // W*H*3 tone-mapped, quantised (and denoised)
 };
 
-// Denoise::bilateralRGB (code/Denoise.cpp:14-86), host side.
-void bilateral_rgb(std::vector<uint8_t>& rgb, int width, int height);
-
 // PNG (RGB8) with tEXt chunks ahead of IDAT (code/Includes/PngText.h:32-63).
 bool write_png(const std::string& path, const uint8_t* rgb, int width, int height,
                const std::vector<std::pair<std::string, std::string>>& text);

@@ -32,6 +32,14 @@ __global__ void k_admit(EngineView E, DRequest r, int slot)
     E.done_flag[slot] = 0;
     E.t_first[slot] = 0ull;
     E.t_done[slot] = 0ull;
+    E.round_state[slot] = 0;
+    E.round_cnt[slot] = 0;
+}
+
+// First adaptive round: every pixel, in order.
+__global__ void k_iota(int* a, int n)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) a[i] = i;
 }
 
 __global__ void k_set_active(EngineView E, ActiveList L)
@@ -129,6 +137,9 @@ Engine::~Engine()
     for (auto& kv : reqs_) {
         Request& r = *kv.second;
         if (r.accum) cudaFreeAsync(r.accum, stream_);
+        for (int k = 0; k < 2; k++)
+            if (r.act[k]) cudaFreeAsync(r.act[k], stream_);
+        if (r.welford) cudaFreeAsync(r.welford, stream_);
         if (r.d_hdr) cudaFreeAsync(r.d_hdr, stream_);
         if (r.d_rgb) cudaFreeAsync(r.d_rgb, stream_);
         if (r.ev_ready) cudaEventDestroy(r.ev_ready);
@@ -165,11 +176,15 @@ void Engine::alloc_buffers()
     d_active_ = dalloc<int>(kMaxActive, T);
     d_nactive_ = dalloc<int>(1, T);
     d_done_ = dalloc<int>(kMaxActive, T);
+    d_round_state_ = dalloc<int>(kMaxActive, T);
+    d_round_cnt_ = dalloc<int>(kMaxActive, T);
     d_cnt_ = dalloc<Counters>(1, T);
     d_params_ = dalloc<EngineParams>(1, T);
     CK(cudaMemset(d_issued_, 0, 8 * kMaxActive));
     CK(cudaMemset(d_outstanding_, 0, 8 * kMaxActive));
     CK(cudaMemset(d_done_, 0, 4 * kMaxActive));
+    CK(cudaMemset(d_round_state_, 0, 4 * kMaxActive));
+    CK(cudaMemset(d_round_cnt_, 0, 4 * kMaxActive));
     CK(cudaMemset(d_nactive_, 0, 4));
     CK(cudaMemset(d_cnt_, 0, sizeof(Counters)));
     for (auto& h : h_snaps_) {
@@ -270,6 +285,8 @@ EngineView Engine::view() const
     E.shadow_cap = shadow_cap_;
     E.queue_cap = queue_cap_;
     E.n_mats = mat_count_;
+    E.round_state = d_round_state_;
+    E.round_cnt = d_round_cnt_;
     return E;
 }
 
@@ -619,10 +636,15 @@ void Engine::validate(int scene, const pcr_render_desc& d) const
         throw PcrError(PCR_ERR_INVALID, "shadow samples exceed the shadow queue sizing");
 }
 
+// Adaptive sampling runs only with more than one aa sample per pixel (the
+// convergence test needs 4 rounds; with aa = 1 there is a single round).
+static bool adaptive_rounds(const pcr_render_desc& d) { return d.adaptive && d.aa_samples > 1; }
+
 int64_t Engine::request_bytes(const pcr_render_desc& d) const
 {
     const int64_t px = (int64_t)d.width * d.height;
-    return px * 3 * (8 + 4 + 1);
+    // accumulator, HDR, 8-bit (+ Welford state and two pixel lists when adaptive)
+    return px * 3 * (8 + 4 + 1) + (adaptive_rounds(d) ? px * (32 + 8) : 0);
 }
 
 int64_t Engine::submit(int scene, const pcr_render_desc& desc)
@@ -679,6 +701,21 @@ void Engine::activate(Request& r, int slot)
     R.seed_hi = (uint32_t)(seed >> 32) ^ (uint32_t)(seed * 0xD1B54A32D192ED03ull >> 17);
     R.total = px * R.paths_per_pixel;
     R.accum = r.accum;
+    if (adaptive_rounds(d)) {
+        R.flags |= kReqAdaptive;
+        CK(cudaMallocFromPoolAsync(&r.act[0], px * sizeof(int), pool_, stream_));
+        CK(cudaMallocFromPoolAsync(&r.act[1], px * sizeof(int), pool_, stream_));
+        CK(cudaMallocFromPoolAsync(&r.welford, px * 2 * sizeof(float4), pool_, stream_));
+        CK(cudaMemsetAsync(r.welford, 0, px * 2 * sizeof(float4), stream_));
+        k_iota<<<std::max<int64_t>(1, std::min<int64_t>((px + 255) / 256, (int64_t)sms_ * 8)), 256, 0, stream_>>>(
+            r.act[0], (int)px);
+        R.act[0] = r.act[0];
+        R.act[1] = r.act[1];
+        R.welford = r.welford;
+        R.round = 0;
+        R.round_base = 0;
+        R.total = px * R.spp;  // round 0 only; each round end adds the next
+    }
     k_admit<<<1, 1, 0, stream_>>>(view(), R, slot);
     CK(cudaGetLastError());
     r.slot = slot;
@@ -742,6 +779,7 @@ void Engine::launch_iteration(int cur, bool prof)
     k_shadow<<<grid_shadow_, B, 0, stream_>>>(E);
     if (prof) CK(cudaEventRecord(prof_ev_[5], stream_));
     k_status<<<1, 1024, 0, stream_>>>(E, cur ^ 1);
+    k_round<<<grid_round_, 256, 0, stream_>>>(E);
     if (prof) CK(cudaEventRecord(prof_ev_[6], stream_));
     CK(cudaGetLastError());
     if (prof) {
@@ -757,6 +795,7 @@ void Engine::launch_iteration(int cur, bool prof)
     } else {
         for (int k : {0, 1, 2, 3, 5, 6}) stage_launches_[k]++;
     }
+    stage_launches_[7]++;  // k_round (timed with k_status)
     iterations_++;
 }
 
@@ -772,6 +811,7 @@ void Engine::build_graph()
     grid_for((const void*)k_extend, B, 0, &grid_extend_);
     grid_for((const void*)k_shade, kShadeBlock, shade_smem_, &grid_shade_);
     grid_for((const void*)k_shadow, B, 0, &grid_shadow_);
+    grid_for((const void*)k_round, 256, 0, &grid_round_);
     if (graph_exec_) {
         cudaGraphExecDestroy(graph_exec_);
         graph_exec_ = nullptr;
@@ -784,7 +824,7 @@ void Engine::build_graph()
         CK(cudaGraphInstantiate(&graph_exec_, g, 0));
         CK(cudaGraphDestroy(g));
         // capture counted launches that did not run
-        for (int k : {0, 1, 2, 3, 5, 6}) stage_launches_[k] -= tune_.iters_per_launch;
+        for (int k : {0, 1, 2, 3, 5, 6, 7}) stage_launches_[k] -= tune_.iters_per_launch;
         iterations_ -= tune_.iters_per_launch;
     }
     graph_dirty_ = false;
@@ -795,7 +835,7 @@ void Engine::launch_block()
     if (graph_dirty_) build_graph();
     if (use_graph_ && !profile_) {
         CK(cudaGraphLaunch(graph_exec_, stream_));
-        for (int k : {0, 1, 2, 3, 5, 6}) stage_launches_[k] += tune_.iters_per_launch;
+        for (int k : {0, 1, 2, 3, 5, 6, 7}) stage_launches_[k] += tune_.iters_per_launch;
         iterations_ += tune_.iters_per_launch;
     } else {
         for (int it = 0; it < tune_.iters_per_launch; it++) launch_iteration(it & 1, profile_);
@@ -813,14 +853,25 @@ void Engine::finish_request(Request& r)
 {
     const pcr_render_desc& d = r.desc;
     const int64_t px = (int64_t)d.width * d.height;
-    const double inv = 1.0 / ((double)d.samples * std::max(1, d.aa_samples));
+    // adaptive requests hold each pixel's final mean already
+    const double inv = adaptive_rounds(d) ? 1.0 : 1.0 / ((double)d.samples * std::max(1, d.aa_samples));
     int grid = std::min<int64_t>((px + 255) / 256, (int64_t)sms_ * 8);
     k_resolve<<<std::max(1, grid), 256, 0, stream_>>>(r.accum, (int)px, inv, d.spectral ? 1 : 0, d.aces ? 1 : 0,
                                                        r.d_hdr, r.d_rgb);
     CK(cudaGetLastError());
+    if (d.denoise) {
+        // two bilateral passes on the 8-bit image, the accumulator as scratch
+        unsigned char* tmp = reinterpret_cast<unsigned char*>(r.accum);
+        k_bilateral<<<std::max(1, grid), 256, 0, stream_>>>(r.d_rgb, tmp, d.width, d.height);
+        k_bilateral<<<std::max(1, grid), 256, 0, stream_>>>(tmp, r.d_rgb, d.width, d.height);
+        CK(cudaGetLastError());
+    }
     // the resolved images stay on the device until fetch copies them out
     CK(cudaFreeAsync(r.accum, stream_));
     r.accum = nullptr;
+    for (int k = 0; k < 2; k++)
+        if (r.act[k]) { CK(cudaFreeAsync(r.act[k], stream_)); r.act[k] = nullptr; }
+    if (r.welford) { CK(cudaFreeAsync(r.welford, stream_)); r.welford = nullptr; }
     if (!r.ev_ready) CK(cudaEventCreateWithFlags(&r.ev_ready, cudaEventDisableTiming));
     CK(cudaEventRecord(r.ev_ready, stream_));
     r.state = ReqState::Resolving;
@@ -866,7 +917,7 @@ void Engine::harvest(bool)
         if (h_snap_->done[s] && h_snap_block_ > r.admit_block) {
             const unsigned long long tf = h_snap_->tf[s], td = h_snap_->td[s];
             r.device_ms = (td > tf && tf) ? (double)(td - tf) * 1e-6 : 0.0;
-            r.paths = (uint64_t)r.desc.width * r.desc.height * r.desc.samples * std::max(1, r.desc.aa_samples);
+            r.paths = h_snap_->issued[s];  // adaptive requests trace fewer than W*H*spp*aa
             finish_request(r);
             slot_owner_[s] = -1;
             bytes_in_use_ -= r.bytes;
@@ -928,6 +979,7 @@ bool Engine::engine_step()
     CK(cudaMemcpyAsync(hs->done, d_done_, sizeof(int) * kMaxActive, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(hs->tf, d_tfirst_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(hs->td, d_tdone_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(hs->issued, d_issued_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
     CK(cudaEventRecord(ev_snaps_[b], stream_));
     snap_next_ = (snap_next_ + 1) % kSnapRing;
     snap_inflight_++;
@@ -1084,6 +1136,19 @@ void Engine::cancel(int64_t id)
 // ---------------------------------------------------------------- plain method
 void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, uint8_t* rgb, pcr_render_stats* st)
 {
+    if (adaptive_rounds(desc)) {
+        // adaptive rounds are opened on the device between iterations: the
+        // request runs alone through the batched loop
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            if (!active_slots_.empty() || !pending_.empty() || serving_)
+                throw PcrError(PCR_ERR_INVALID, "plain render while batched work is active");
+        }
+        const int64_t id = submit(scene, desc);
+        run_until_idle();
+        fetch(id, hdr, rgb, st);
+        return;
+    }
     std::lock_guard<std::mutex> g(run_mu_);
     CK(cudaSetDevice(device_));
     validate(scene, desc);
@@ -1244,6 +1309,8 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
         throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: more than " + std::to_string(kNoAllocShadowPerVertex) +
                                             " shadow samples per hit");
     if (!hdr_dev && !rgb_dev) throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: no output buffer");
+    if (adaptive_rounds(desc))
+        throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc: adaptive sampling needs per-pixel state; use pcr_render");
     if (!active_slots_.empty() || serving_)
         throw PcrError(PCR_ERR_INVALID, "pcr_render_noalloc while batched work is active");
 
@@ -1268,6 +1335,8 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     int* active = reinterpret_cast<int*>(take(4));
     int* n_active = reinterpret_cast<int*>(take(4));
     int* done = reinterpret_cast<int*>(take(4));
+    int* round_state = reinterpret_cast<int*>(take(4));
+    int* round_cnt = reinterpret_cast<int*>(take(4));
     const size_t header_used = off;
     off = kNoAllocHeader;
     PathQueue q[2];
@@ -1314,6 +1383,8 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     E.sq = sq;
     E.give_start = give_start;
     E.shadow_cap = kNoAllocShadow;
+    E.round_state = round_state;
+    E.round_cnt = round_cnt;
     E.queue_cap = kNoAllocQueue;
     E.n_mats = mat_count_;
 
@@ -1368,6 +1439,13 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     k_resolve<<<std::max(1, grid), 256, 0, stream_>>>(accum, (int)px, inv, desc.spectral ? 1 : 0, desc.aces ? 1 : 0,
                                                        hdr_dev, rgb_dev);
     CK(cudaGetLastError());
+    if (desc.denoise && rgb_dev) {
+        // two bilateral passes; the accumulator region (24 B a pixel) is free now
+        unsigned char* tmp = reinterpret_cast<unsigned char*>(accum);
+        k_bilateral<<<std::max(1, grid), 256, 0, stream_>>>(rgb_dev, tmp, desc.width, desc.height);
+        k_bilateral<<<std::max(1, grid), 256, 0, stream_>>>(tmp, rgb_dev, desc.width, desc.height);
+        CK(cudaGetLastError());
+    }
     CK(cudaStreamSynchronize(stream_));
 }
 

@@ -53,6 +53,8 @@ struct Request {
     double device_ms = 0;
     uint64_t paths = 0;
     uint64_t admit_block = 0;  // blocks launched before this request's slot was (re)set
+    int* act[2] = {nullptr, nullptr};   // adaptive: pixel lists of alternate rounds
+    float4* welford = nullptr;          // adaptive: per-pixel mean / M2
 };
 
 struct EngineTuning {
@@ -146,9 +148,14 @@ private:
     long long* d_outstanding_ = nullptr;
     long long* d_give_start_ = nullptr;
     int *d_give_ = nullptr, *d_give_base_ = nullptr, *d_active_ = nullptr, *d_nactive_ = nullptr, *d_done_ = nullptr;
+    int *d_round_state_ = nullptr, *d_round_cnt_ = nullptr;
     int* h_active_ = nullptr;     // pinned: [0] = n, then slots
     Counters* d_cnt_ = nullptr;
-    struct HostSnap { Counters cnt; int done[kMaxActive]; unsigned long long tf[kMaxActive], td[kMaxActive]; };
+    struct HostSnap {
+        Counters cnt;
+        int done[kMaxActive];
+        unsigned long long tf[kMaxActive], td[kMaxActive], issued[kMaxActive];
+    };
     // Device state copied out after each block of iterations, into a ring of
     // pinned buffers: the host keeps up to kSnapRing blocks queued and
     // harvests each block's copy once it has landed, so the GPU does not idle
@@ -176,7 +183,7 @@ private:
     // graph
     cudaGraphExec_t graph_exec_ = nullptr;
     bool graph_dirty_ = true;
-    int grid_regen_ = 0, grid_extend_ = 0, grid_shade_ = 0, grid_shadow_ = 0;
+    int grid_regen_ = 0, grid_extend_ = 0, grid_shade_ = 0, grid_shadow_ = 0, grid_round_ = 0;
     size_t shade_smem_ = 0;
     int smem_mats_ = 0;
 

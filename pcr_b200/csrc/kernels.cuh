@@ -51,6 +51,23 @@ __global__ void __launch_bounds__(kSchedThreads) k_schedule(EngineView E, const 
     long long rem = 0;
     if (tid < n_act) {
         slot = E.active[tid];
+        if (E.round_state[slot] == 1) {
+            // an adaptive round ended last iteration and k_round kept
+            // round_cnt pixels: open the next round, or finish the request
+            DRequest& R = const_cast<DRequest&>(E.reqs[slot]);
+            const int kept = E.round_cnt[slot];
+            E.round_cnt[slot] = 0;
+            E.round_state[slot] = 0;
+            R.round_base = R.total;
+            R.round += 1;
+            R.total += (long long)kept * R.spp;
+            if (kept == 0) {
+                unsigned long long t;
+                asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+                E.done_flag[slot] = 1;
+                E.t_done[slot] = t;
+            }
+        }
         rem = E.reqs[slot].total - (long long)E.issued[slot];
         if (rem < 0) rem = 0;
     }
@@ -222,8 +239,17 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
         const int slot = s_slot[lo];
         const DRequest& R = E.reqs[slot];
         const long long path = s_start[lo] + (i - s_base[lo]);
-        const uint32_t pixel = (uint32_t)(path / R.paths_per_pixel);
-        const uint32_t sample = (uint32_t)(path % R.paths_per_pixel);
+        uint32_t pixel, sample;
+        if (R.flags & kReqAdaptive) {
+            // round r: spp paths for each pixel still in the round's list;
+            // sample numbers r*spp.. as in the non-adaptive order
+            const long long q = path - R.round_base;
+            pixel = (uint32_t)R.act[R.round & 1][q / R.spp];
+            sample = (uint32_t)(R.round * R.spp + (int)(q % R.spp));
+        } else {
+            pixel = (uint32_t)(path / R.paths_per_pixel);
+            sample = (uint32_t)(path % R.paths_per_pixel);
+        }
         const int px = (int)(pixel % (uint32_t)R.width), py = (int)(pixel / (uint32_t)R.width);
         float jx = 0.f, jy = 0.f;
         if (R.aa > 1) {
@@ -759,10 +785,16 @@ __global__ void k_status(EngineView E, int next)
     for (int r = threadIdx.x; r < n_act; r += blockDim.x) {
         const int slot = E.active[r];
         if (E.done_flag[slot]) continue;
+        if (E.round_state[slot]) { s_busy = 1; continue; }
         const bool all_issued = (long long)E.issued[slot] >= E.reqs[slot].total;
         if (all_issued && E.outstanding[slot] == 0) {
-            E.done_flag[slot] = 1;
-            E.t_done[slot] = now;
+            if (E.reqs[slot].flags & kReqAdaptive) {
+                E.round_state[slot] = 1;  // k_round, then the next k_schedule
+                s_busy = 1;
+            } else {
+                E.done_flag[slot] = 1;
+                E.t_done[slot] = now;
+            }
         } else {
             s_busy = 1;
         }
@@ -771,6 +803,63 @@ __global__ void k_status(EngineView E, int next)
     if (threadIdx.x == 0) {
         C->idle = (s_busy == 0 && C->queue_n[next] == 0) ? 1 : 0;
         C->iter++;
+    }
+}
+
+// ------------------------------------------------------------------ adaptive rounds
+// End of an adaptive aa round (the GPU backends' per-pixel Welford loop,
+// code/Gpu/Opengl/OpenglRenderer.cpp:1288-1383): each pixel of the round
+// takes the mean of its spp paths, updates its running mean / M2, and stops
+// after 4 or more rounds once every channel's relative variance
+// M2/(taken-1) / (mean^2 + 0.01) is below 0.05, or after aa rounds.
+// Stopped pixels write their mean to the accumulator (resolved with weight
+// 1); the others reset it and move to the next round's list.
+__global__ void k_round(EngineView E)
+{
+    const int n_act = *E.n_active;
+    const int lane = threadIdx.x & 31;
+    for (int r = 0; r < n_act; r++) {
+        const int slot = E.active[r];
+        if (E.round_state[slot] != 1) continue;
+        const DRequest& R = E.reqs[slot];
+        const int n = (int)((R.total - R.round_base) / R.spp);
+        const int* list = R.act[R.round & 1];
+        int* next = R.act[(R.round & 1) ^ 1];
+        const float inv = 1.f / (float)R.spp;
+        const int stride = gridDim.x * blockDim.x;
+        for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {  // warp-uniform trips
+            const int k = base + threadIdx.x;
+            bool keep = false;
+            int px = 0;
+            if (k < n) {
+                px = list[k];
+                double* a = R.accum + (size_t)px * 3;
+                const float3 c = make_float3((float)a[0] * inv, (float)a[1] * inv, (float)a[2] * inv);
+                float4 m = R.welford[2 * (size_t)px], m2 = R.welford[2 * (size_t)px + 1];
+                const float taken = m.w + 1.f;
+                const float3 d1 = make_float3(c.x - m.x, c.y - m.y, c.z - m.z);
+                m.x += d1.x / taken; m.y += d1.y / taken; m.z += d1.z / taken;
+                const float3 d2 = make_float3(c.x - m.x, c.y - m.y, c.z - m.z);
+                m2.x += d1.x * d2.x; m2.y += d1.y * d2.y; m2.z += d1.z * d2.z;
+                m.w = taken;
+                bool done = (int)taken >= R.aa;
+                if (!done && taken >= 4.f) {
+                    const float t1 = taken - 1.f;
+                    const float rx = (m2.x / t1) / (m.x * m.x + 0.01f), ry = (m2.y / t1) / (m.y * m.y + 0.01f),
+                                rz = (m2.z / t1) / (m.z * m.z + 0.01f);
+                    done = fmaxf(fmaxf(rx, ry), rz) < 0.05f;
+                }
+                R.welford[2 * (size_t)px] = m;
+                R.welford[2 * (size_t)px + 1] = m2;
+                if (done) { a[0] = m.x; a[1] = m.y; a[2] = m.z; }
+                else { a[0] = 0.0; a[1] = 0.0; a[2] = 0.0; keep = true; }
+            }
+            const unsigned km = __ballot_sync(0xffffffffu, keep);
+            int b = 0;
+            if (lane == 0 && km) b = atomicAdd(&E.round_cnt[slot], __popc(km));
+            b = __shfl_sync(0xffffffffu, b, 0);
+            if (keep) next[b + __popc(km & ((1u << lane) - 1u))] = px;
+        }
     }
 }
 
@@ -789,6 +878,52 @@ __global__ void k_resolve(const double* __restrict__ acc, int npix, double inv_n
             rgb8[i * 3] = quantize(m.x);
             rgb8[i * 3 + 1] = quantize(m.y);
             rgb8[i * 3 + 2] = quantize(m.z);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ denoise
+// One pass of the 5x5 cross-bilateral on the 8-bit image (Denoise::
+// bilateralRGB, code/Denoise.cpp:14-86, which runs two): spatial sigma 1.5
+// px, colour sigma 10 levels, float arithmetic in the reference's order (no
+// contraction), the weight's exponential taken in double and rounded once.
+__global__ void k_bilateral(const unsigned char* __restrict__ src, unsigned char* __restrict__ dst, int width,
+                            int height)
+{
+    using namespace ex;
+    const float invSpatial2 = div(1.0f, mul(mul(2.0f, 1.5f), 1.5f));
+    const float invColor2 = div(1.0f, mul(mul(2.0f, 10.0f), 10.0f));
+    const int npix = width * height;
+    for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < npix; p += gridDim.x * blockDim.x) {
+        const int y = p / width, x = p - y * width;
+        const float cR = (float)src[p * 3], cG = (float)src[p * 3 + 1], cB = (float)src[p * 3 + 2];
+        float sumW = 0.f, sumR = 0.f, sumG = 0.f, sumB = 0.f;
+        for (int dy = -2; dy <= 2; dy++) {
+            const int ny = y + dy;
+            if (ny < 0 || ny >= height) continue;
+            for (int dx = -2; dx <= 2; dx++) {
+                const int nx = x + dx;
+                if (nx < 0 || nx >= width) continue;
+                const int q = (ny * width + nx) * 3;
+                const float nR = (float)src[q], nG = (float)src[q + 1], nB = (float)src[q + 2];
+                const float spatial = mul((float)(dx * dx + dy * dy), invSpatial2);
+                const float dR = sub(nR, cR), dG = sub(nG, cG), dB = sub(nB, cB);
+                const float color = mul(add(add(mul(dR, dR), mul(dG, dG)), mul(dB, dB)), invColor2);
+                const float w = (float)exp(-(double)add(spatial, color));
+                sumW = add(sumW, w);
+                sumR = add(sumR, mul(w, nR));
+                sumG = add(sumG, mul(w, nG));
+                sumB = add(sumB, mul(w, nB));
+            }
+        }
+        if (sumW > 0.f) {
+            dst[p * 3] = (unsigned char)fminf(255.f, add(div(sumR, sumW), 0.5f));
+            dst[p * 3 + 1] = (unsigned char)fminf(255.f, add(div(sumG, sumW), 0.5f));
+            dst[p * 3 + 2] = (unsigned char)fminf(255.f, add(div(sumB, sumW), 0.5f));
+        } else {
+            dst[p * 3] = src[p * 3];
+            dst[p * 3 + 1] = src[p * 3 + 1];
+            dst[p * 3 + 2] = src[p * 3 + 2];
         }
     }
 }

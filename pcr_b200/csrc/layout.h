@@ -110,7 +110,7 @@ struct DScene {
 };
 
 // Request flags
-constexpr int kReqSpectral = 1, kReqMIS = 2, kReqRussian = 4, kReqStratified = 8;
+constexpr int kReqSpectral = 1, kReqMIS = 2, kReqRussian = 4, kReqStratified = 8, kReqAdaptive = 16;
 
 struct DRequest {
     int scene, width, height, depth;
@@ -118,8 +118,18 @@ struct DRequest {
     int spp, aa, shadow, flags, hero, strata;
     float cam_x, cam_y, cam_z, scale, aspect;
     uint32_t seed_lo, seed_hi;
-    long long total;          // width * height * paths_per_pixel
+    long long total;          // width * height * paths_per_pixel (adaptive: paths issued through this round)
     double* accum;            // width * height * 3
+    // Adaptive sampling (kReqAdaptive): the aa samples run as rounds; round
+    // r traces spp paths for each pixel still in act[r & 1].  Per pixel the
+    // round's mean enters a Welford mean / M2 (welford[2p] = mean, taken;
+    // welford[2p+1] = M2); converged or finished pixels leave the list and
+    // their final mean goes to accum.
+    int* act[2];
+    float4* welford;
+    long long round_base;     // paths issued before this round
+    int round;
+    int pad_;
 };
 
 // Path state, structure of arrays, one entry per queued path.
@@ -175,6 +185,8 @@ struct EngineView {
     int shadow_cap;                  // shadow-queue entries
     int queue_cap;                   // entries per path queue
     int n_mats;
+    int* round_state;                // per slot: 1 while an adaptive round's per-pixel step is pending
+    int* round_cnt;                  // per slot: pixels kept for the next adaptive round
 };
 
 }  // namespace pcr
