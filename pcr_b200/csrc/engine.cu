@@ -178,6 +178,7 @@ void Engine::alloc_buffers()
     d_done_ = dalloc<int>(kMaxActive, T);
     d_round_state_ = dalloc<int>(kMaxActive, T);
     d_round_cnt_ = dalloc<int>(kMaxActive, T);
+    d_round_list_ = dalloc<int>(kMaxActive, T);
     d_cnt_ = dalloc<Counters>(1, T);
     d_params_ = dalloc<EngineParams>(1, T);
     CK(cudaMemset(d_issued_, 0, 8 * kMaxActive));
@@ -287,6 +288,7 @@ EngineView Engine::view() const
     E.n_mats = mat_count_;
     E.round_state = d_round_state_;
     E.round_cnt = d_round_cnt_;
+    E.round_list = d_round_list_;
     return E;
 }
 
@@ -811,7 +813,7 @@ void Engine::build_graph()
     grid_for((const void*)k_extend, B, 0, &grid_extend_);
     grid_for((const void*)k_shade, kShadeBlock, shade_smem_, &grid_shade_);
     grid_for((const void*)k_shadow, B, 0, &grid_shadow_);
-    grid_for((const void*)k_round, 256, 0, &grid_round_);
+    grid_round_ = sms_ * 2;  // a round's per-pixel step is light; an idle launch reads one word
     if (graph_exec_) {
         cudaGraphExecDestroy(graph_exec_);
         graph_exec_ = nullptr;
@@ -1337,6 +1339,7 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     int* done = reinterpret_cast<int*>(take(4));
     int* round_state = reinterpret_cast<int*>(take(4));
     int* round_cnt = reinterpret_cast<int*>(take(4));
+    int* round_list = reinterpret_cast<int*>(take(4));
     const size_t header_used = off;
     off = kNoAllocHeader;
     PathQueue q[2];
@@ -1385,6 +1388,7 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     E.shadow_cap = kNoAllocShadow;
     E.round_state = round_state;
     E.round_cnt = round_cnt;
+    E.round_list = round_list;
     E.queue_cap = kNoAllocQueue;
     E.n_mats = mat_count_;
 

@@ -105,6 +105,7 @@ __global__ void __launch_bounds__(kSchedThreads) k_schedule(EngineView E, const 
     if (tid == 0) s_total = totg;
     __syncthreads();
     if (tid == 0) {
+        C->n_rounds = 0;  // k_round of the last iteration has read the list
         C->new_base = qn;
         C->new_n = (int)s_total;
         C->queue_n[cur] = qn + (int)s_total;
@@ -790,6 +791,7 @@ __global__ void k_status(EngineView E, int next)
         if (all_issued && E.outstanding[slot] == 0) {
             if (E.reqs[slot].flags & kReqAdaptive) {
                 E.round_state[slot] = 1;  // k_round, then the next k_schedule
+                E.round_list[atomicAdd(&C->n_rounds, 1)] = slot;
                 s_busy = 1;
             } else {
                 E.done_flag[slot] = 1;
@@ -816,11 +818,10 @@ __global__ void k_status(EngineView E, int next)
 // 1); the others reset it and move to the next round's list.
 __global__ void k_round(EngineView E)
 {
-    const int n_act = *E.n_active;
+    const int n_rounds = E.cnt->n_rounds;
     const int lane = threadIdx.x & 31;
-    for (int r = 0; r < n_act; r++) {
-        const int slot = E.active[r];
-        if (E.round_state[slot] != 1) continue;
+    for (int r = 0; r < n_rounds; r++) {
+        const int slot = E.round_list[r];
         const DRequest& R = E.reqs[slot];
         const int n = (int)((R.total - R.round_base) / R.spp);
         const int* list = R.act[R.round & 1];

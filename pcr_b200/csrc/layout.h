@@ -160,6 +160,7 @@ struct Counters {
     int iter;
     int status;           // non-zero: a kernel reported an error
     int idle;             // 1 when no request has work left
+    int n_rounds;         // adaptive requests whose round ended this iteration (k_status -> k_round)
     unsigned long long rays, shadow_rays, paths;
 };
 
@@ -187,6 +188,7 @@ struct EngineView {
     int n_mats;
     int* round_state;                // per slot: 1 while an adaptive round's per-pixel step is pending
     int* round_cnt;                  // per slot: pixels kept for the next adaptive round
+    int* round_list;                 // slots of Counters::n_rounds
 };
 
 }  // namespace pcr
