@@ -61,6 +61,8 @@ def args_():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-matched", action="store_true")
     p.add_argument("--queue", type=int, default=0, help="paths in flight (0: library default)")
+    p.add_argument("--no-autotune", action="store_true",
+                   help="skip the autotuner (queue size, block size, issue chunk, refill cadence)")
     p.add_argument("--serve-requests", type=int, default=400)
     p.add_argument("--serve-rate", type=float, default=200.0)
     return p.parse_args()
@@ -337,6 +339,14 @@ def main():
     descs = [capi.render_desc(r["width"], r["height"], depth=r["depth"], samples=r["samples"], shadow=r["shadow"],
                               spectral=True, seed=r["seed"]) for r in batch]
     step_paths = sum(r["width"] * r["height"] * r["samples"] for r in batch)
+    autotune = None
+    if not a.no_autotune and not a.queue:
+        # the library's autotuner times a grid of tunings on a sample of the
+        # batch (every 4th render) and keeps the fastest for the run
+        sub = list(range(0, len(batch), 4))
+        t0 = time.perf_counter()
+        chosen = ctx.autotune([sids[batch[k]["variant"]] for k in sub], [descs[k] for k in sub])
+        autotune = {"chosen": chosen, "sample_renders": len(sub), "seconds": time.perf_counter() - t0}
 
     def batched_step(want_images=False):
         ids = [ctx.submit(sids[r["variant"]], d) for r, d in zip(batch, descs)]
@@ -398,7 +408,8 @@ def main():
     # ---- per-stage events (profiled pass) for the roofline
     roofline = None
     if not a.no_profile:
-        pctx = capi.Context(device=local, profile=True, queue_capacity=a.queue)
+        tune = {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")}
+        pctx = capi.Context(device=local, profile=True, **tune)
         psids = {v: pctx.load_scene_json(p, data) for v, p in files.items()}
         ids = [pctx.submit(psids[r["variant"]], d) for r, d in zip(batch, descs)]
         pctx.run_until_idle()
@@ -471,6 +482,7 @@ def main():
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
             "serve": serve, "matched_rmse": matched,
             "tuning": {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")},
+            "autotune": autotune,
         }
         print(json.dumps(out))
     ctx.close()
