@@ -414,6 +414,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
     // block-uniform trip count: every thread of a block runs the same
     // iterations, so the block-wide append at the bottom sees all of them
     __shared__ int s_app[2][kShadeBlock / 32 + 1];
+    __shared__ int s_shd[2][kShadeBlock / 32 + 1];
     int parity = 0;
     const int stride = gridDim.x * blockDim.x;
     for (int base = blockIdx.x * blockDim.x; base < n; base += stride) {
@@ -439,6 +440,44 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
         float3 emit_xyz = make_float3(0, 0, 0);
         bool emit = false;
         bool spec_path = false;
+
+        // Shadow records: a diffuse vertex with a light in its scene writes
+        // R.shadow of them.  They are reserved for the whole block at once
+        // (one contiguous range, its warps in order), so k_shadow's warps
+        // rarely straddle two blocks' records, which may belong to
+        // different scenes.
+        int nee = 0;
+        if (live && (prim & kPrimKindMask) != kPrimNone) {
+            const DScene& S0 = E.scenes[id.w];
+            if (S0.total_light_area > 0.f) {
+                const uint32_t k0 = prim & kPrimKindMask, p0 = prim & kPrimIndexMask;
+                const int mi0 = k0 == kPrimSphere ? S0.spheres[p0].mat.x
+                              : k0 == kPrimPlane  ? __float_as_int(S0.planes[p0].o_mat.w)
+                                                  : __float_as_int(S0.tris[p0].e1_mat.w);
+                if (!(M[S0.mat_base + mi0].flags & (kMatEmissive | kMatMetallic | kMatTransparent)))
+                    nee = E.reqs[slot].shadow;
+            }
+        }
+        int spos_block;
+        {
+            int ex = nee;  // inclusive scan across the warp
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int v = __shfl_up_sync(0xffffffffu, ex, off);
+                if (lane >= off) ex += v;
+            }
+            int* sw = s_shd[parity];
+            const int wid = threadIdx.x >> 5;
+            if (lane == 31) sw[wid] = ex;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                int tot = 0;
+                for (int k = 0; k < kShadeBlock / 32; k++) { const int c = sw[k]; sw[k] = tot; tot += c; }
+                sw[kShadeBlock / 32] = tot ? atomicAdd(&C->shadow_n, tot) : 0;
+            }
+            __syncthreads();
+            spos_block = sw[kShadeBlock / 32] + sw[wid] + ex - nee;
+        }
 
         if (live && (prim & kPrimKindMask) != kPrimNone) {
             const DRequest& R = E.reqs[slot];
@@ -597,7 +636,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         V = f3mul(apply_xyz(load_weights(Q, i), tpal), scaleS);
                         cached = S.emit_mat;
                     }
-                    const int spos = group_append(&C->shadow_n, R.shadow);
+                    const int spos = spos_block;
                     const int nsh = spos + R.shadow <= E.shadow_cap ? R.shadow : 0;
                     if (nsh == 0) atomicOr(&C->status, 1);
                     for (int s = 0; s < nsh; s++) {
