@@ -185,6 +185,35 @@ def test_shadow_test_matches_oracle_on_mesh(ctx, O, mesh):
     assert want.mean() > 0.05
 
 
+def test_bvh_hit_ids_on_1m_triangle_mesh(ctx, O):
+    """The serving-at-scale mesh: a seeded displaced icosphere of 1,003,520
+    triangles.  The host-built tree equals the oracle's restatement of the
+    reference builder node for node, and 2M seeded rays hit the same
+    triangle ids through the 4-wide device BVH (t-ties within 1e-6 aside)."""
+    from pcr_b200 import capi, workloads
+    path = workloads.mesh_scene(224, 3)
+    hs = capi.HostScene(path, GOLDEN)
+    tl = hs.triangles()
+    ids = hs.triangle_ids()
+    tris = np.zeros((tl.shape[0], 9), np.float32)
+    tris[ids] = tl[:, :9]
+    assert tris.shape[0] == 1_003_520
+    boxes, ints, perm, arr, nodes = O.bvh_build(tris)
+    b = hs.bvh()
+    assert np.array_equal(b[:, :6].view(np.uint32), boxes.view(np.uint32))
+    assert np.array_equal(b[:, 6:].view(np.int32), ints)
+    sid = ctx.load_scene_json(path, GOLDEN)
+    rays = box_rays(2_000_000, 224)
+    gid, gt = ctx.trace_bvh(sid, rays)
+    oid, ot = _oracle_bvh_query(O, nodes, arr, rays)
+    assert np.array_equal(gid >= 0, oid >= 0), "hit/miss disagreement"
+    bad = (gid != oid) & ~(np.abs(gt - ot) <= 1e-6)
+    assert bad.sum() == 0, f"{bad.sum()} id mismatches outside t-ties"
+    assert (gid >= 0).mean() > 0.05
+    ctx.release_scene(sid)
+    hs.close()
+
+
 def test_bvh_counts_match_reference_traversal_order_of_magnitude(ctx, O, mesh):
     rays = box_rays(65536, 3)
     _, _, cnt = ctx.trace_bvh(mesh["sid"], rays, counts=True)
