@@ -234,6 +234,29 @@ pcr_status pcr_trace_closest(pcr_ctx *ctx, pcr_scene_id scene, const float *rays
  * per-ray counts of internal nodes visited and triangles tested (may be NULL). */
 pcr_status pcr_trace_bvh(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, int64_t n,
                          int32_t *tri_id, float *t, int32_t *counts);
+/* ------------------------------------------------------------- router
+ * Request router over several contexts, typically one per GPU of a node
+ * (the scale-out of the serving path; the reference renders on one device
+ * and has no counterpart).  The router borrows the contexts (they must
+ * outlive it), replicates scenes into each one's scene cache, and sends
+ * each request to the context with the fewest paths outstanding (submitted
+ * and not yet fetched).  Requests are independent, so there is no data
+ * exchange between devices; a request's image is the same whichever
+ * context renders it.  Tickets name (context, request).  Thread-safe. */
+typedef struct pcr_router pcr_router;
+pcr_status pcr_router_create(pcr_router **out, pcr_ctx *const *ctxs, int32_t n);
+pcr_status pcr_router_destroy(pcr_router *r);
+pcr_status pcr_router_scene_load_json(pcr_router *r, const char *path, const char *data_root,
+                                      const char *lut_path, pcr_scene_id *out);
+pcr_status pcr_router_serve_start(pcr_router *r);
+pcr_status pcr_router_serve_stop(pcr_router *r);
+pcr_status pcr_router_submit(pcr_router *r, pcr_scene_id scene, const pcr_render_desc *desc, int64_t *ticket);
+pcr_status pcr_router_wait(pcr_router *r, int64_t ticket, int64_t timeout_ms);
+pcr_status pcr_router_fetch(pcr_router *r, int64_t ticket, float *hdr_out, uint8_t *rgb8_out,
+                            pcr_render_stats *stats);
+/* per-context paths outstanding (n entries) and requests routed (n entries) */
+pcr_status pcr_router_load(pcr_router *r, int64_t *outstanding_paths, int64_t *routed);
+
 /* The shadow test of one light sample (code/Renderer.cpp:852-860) on caller
  * rays: rays = n x (origin xyz, unit direction xyz), light_dist2 = squared
  * distance to the light sample; blocked[i] = 1 when the closest hit is

@@ -27,6 +27,8 @@ EXPORTS = [
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
     "pcr_fetch", "pcr_cancel", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
     "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_eval_stage",
+    "pcr_router_create", "pcr_router_destroy", "pcr_router_scene_load_json", "pcr_router_serve_start",
+    "pcr_router_serve_stop", "pcr_router_submit", "pcr_router_wait", "pcr_router_fetch", "pcr_router_load",
 ]
 
 
@@ -153,6 +155,15 @@ def load_library():
         "pcr_trace_closest": [P, C.c_int32, fp, C.c_int64, ip, ip, fp],
         "pcr_trace_bvh": [P, C.c_int32, fp, C.c_int64, ip, fp, ip],
         "pcr_trace_shadow": [P, C.c_int32, fp, fp, C.c_int64, ip],
+        "pcr_router_create": [C.POINTER(P), C.POINTER(P), C.c_int32],
+        "pcr_router_destroy": [P],
+        "pcr_router_scene_load_json": [P, C.c_char_p, C.c_char_p, C.c_char_p, ip],
+        "pcr_router_serve_start": [P],
+        "pcr_router_serve_stop": [P],
+        "pcr_router_submit": [P, C.c_int32, C.POINTER(RenderDesc), C.POINTER(C.c_int64)],
+        "pcr_router_wait": [P, C.c_int64, C.c_int64],
+        "pcr_router_fetch": [P, C.c_int64, fp, C.POINTER(C.c_uint8), C.POINTER(RenderStats)],
+        "pcr_router_load": [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)],
         "pcr_eval_stage": [P, C.c_int32, fp, fp, C.c_int64, fp],
     }
     for name, args in sig.items():
@@ -416,3 +427,63 @@ class Context:
         p = np.ascontiguousarray(params, np.float32) if params is not None else None
         _check(self.L.pcr_eval_stage(self.h, what, _fp(p) if p is not None else None, _fp(x), n, _fp(out)))
         return out
+
+
+class Router:
+    """Request router over several contexts (pcr_router_*): scenes are
+    replicated into every context; each request goes to the context with
+    the fewest paths outstanding.  The contexts must outlive the router."""
+
+    def __init__(self, contexts):
+        self.L = load_library()
+        self.ctxs = list(contexts)
+        arr = (C.c_void_p * len(self.ctxs))(*[c.h.value for c in self.ctxs])
+        h = C.c_void_p()
+        _check(self.L.pcr_router_create(C.byref(h), C.cast(arr, C.POINTER(C.c_void_p)), len(self.ctxs)))
+        self.h = h
+
+    def close(self):
+        if getattr(self, "h", None):
+            _check(self.L.pcr_router_destroy(self.h))
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def load_scene_json(self, path: str, data_root: str | None = None, lut_path: str | None = None) -> int:
+        out = C.c_int32()
+        _check(self.L.pcr_router_scene_load_json(self.h, path.encode(), data_root.encode() if data_root else None,
+                                                 lut_path.encode() if lut_path else None, C.byref(out)))
+        return out.value
+
+    def serve_start(self) -> None:
+        _check(self.L.pcr_router_serve_start(self.h))
+
+    def serve_stop(self) -> None:
+        _check(self.L.pcr_router_serve_stop(self.h))
+
+    def submit(self, sid: int, desc: RenderDesc) -> int:
+        t = C.c_int64()
+        _check(self.L.pcr_router_submit(self.h, sid, C.byref(desc), C.byref(t)))
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1) -> None:
+        _check(self.L.pcr_router_wait(self.h, ticket, timeout_ms))
+
+    def fetch(self, ticket: int, width: int, height: int, want_hdr=True, want_rgb=True):
+        hdr = np.zeros((height, width, 3), np.float32) if want_hdr else None
+        rgb = np.zeros((height, width, 3), np.uint8) if want_rgb else None
+        st = RenderStats()
+        _check(self.L.pcr_router_fetch(self.h, ticket, _fp(hdr) if want_hdr else None,
+                                       rgb.ctypes.data_as(C.POINTER(C.c_uint8)) if want_rgb else None, C.byref(st)))
+        return hdr, rgb, st
+
+    def load(self):
+        n = len(self.ctxs)
+        out = (C.c_int64 * n)()
+        routed = (C.c_int64 * n)()
+        _check(self.L.pcr_router_load(self.h, out, routed))
+        return list(out), list(routed)

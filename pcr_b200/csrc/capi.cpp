@@ -2,8 +2,11 @@
 // this boundary: every entry point converts errors into a pcr_status and a
 // thread-local message (pcr_last_error).
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/pcr_cuda.h"
 #include "engine.h"
@@ -15,6 +18,17 @@ struct pcr_ctx {
 
 struct pcr_host_scene {
     pcr::HostScene s;
+};
+
+// Least-outstanding-paths router over borrowed contexts.
+struct pcr_router {
+    std::vector<pcr::Engine*> eng;
+    std::mutex mu;
+    std::vector<std::vector<int>> scene_map;   // router scene id -> per-context scene id
+    struct Ticket { int ctx; int64_t id; int64_t paths; };
+    std::map<int64_t, Ticket> tickets;
+    std::vector<int64_t> load, routed;
+    int64_t next = 1;
 };
 
 namespace {
@@ -49,6 +63,20 @@ std::string parent_dir(const std::string& p)
 {
     auto k = p.find_last_of('/');
     return k == std::string::npos ? std::string(".") : (k == 0 ? std::string("/") : p.substr(0, k));
+}
+
+pcr::HostScene host_scene_from_json(const char* path, const char* data_root, const char* lut_path)
+{
+    // default data root: the directory that holds the scene directory
+    // (the reference ships <root>/Scenes/*.json beside <root>/spd/)
+    std::string root = data_root ? std::string(data_root) : parent_dir(parent_dir(path));
+    std::vector<float> lut;
+    if (lut_path) {
+        std::string err;
+        if (!pcr::load_plut(lut_path, lut, &err))
+            throw pcr::PcrError(PCR_ERR_SCENE, std::string("loadLUT(") + lut_path + "): " + err);
+    }
+    return pcr::load_scene_json(path, root, lut_path ? &lut : nullptr);
 }
 }  // namespace
 
@@ -100,15 +128,7 @@ pcr_status pcr_scene_load_json(pcr_ctx* ctx, const char* path, const char* data_
 {
     return guard([&] {
         if (!path || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
-        // default data root: the directory that holds the scene directory
-        // (the reference ships <root>/Scenes/*.json beside <root>/spd/)
-        std::string root = data_root ? std::string(data_root) : parent_dir(parent_dir(path));
-        std::vector<float> lut;
-        if (lut_path) {
-            std::string err;
-            if (!pcr::load_plut(lut_path, lut, &err)) throw pcr::PcrError(PCR_ERR_SCENE, std::string("loadLUT(") + lut_path + "): " + err);
-        }
-        pcr::HostScene s = pcr::load_scene_json(path, root, lut_path ? &lut : nullptr);
+        pcr::HostScene s = host_scene_from_json(path, data_root, lut_path);
         pcr_scene_desc d = s.desc();
         *out = E(ctx).upload_scene(d);
     });
@@ -271,6 +291,124 @@ pcr_status pcr_trace_bvh(pcr_ctx* ctx, pcr_scene_id scene, const float* rays, in
     return guard([&] {
         if (!rays && n > 0) throw pcr::PcrError(PCR_ERR_INVALID, "null rays");
         E(ctx).trace(scene, rays, n, nullptr, tri_id, t, 1, counts);
+    });
+}
+
+pcr_status pcr_router_create(pcr_router** out, pcr_ctx* const* ctxs, int32_t n)
+{
+    return guard([&] {
+        if (!out || !ctxs || n <= 0) throw pcr::PcrError(PCR_ERR_INVALID, "router needs at least one context");
+        auto r = std::make_unique<pcr_router>();
+        for (int i = 0; i < n; i++) r->eng.push_back(&E(ctxs[i]));
+        r->load.assign(n, 0);
+        r->routed.assign(n, 0);
+        *out = r.release();
+    });
+}
+
+pcr_status pcr_router_destroy(pcr_router* r)
+{
+    return guard([&] { delete r; });
+}
+
+namespace {
+pcr_router& RT(pcr_router* r)
+{
+    if (!r) throw pcr::PcrError(PCR_ERR_INVALID, "null router");
+    return *r;
+}
+}  // namespace
+
+pcr_status pcr_router_scene_load_json(pcr_router* r, const char* path, const char* data_root, const char* lut_path,
+                                      pcr_scene_id* out)
+{
+    return guard([&] {
+        pcr_router& R = RT(r);
+        if (!path || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        pcr::HostScene hs = host_scene_from_json(path, data_root, lut_path);
+        const pcr_scene_desc d = hs.desc();
+        std::vector<int> ids;
+        for (pcr::Engine* e : R.eng) ids.push_back(e->upload_scene(d));
+        std::lock_guard<std::mutex> g(R.mu);
+        R.scene_map.push_back(ids);
+        *out = (pcr_scene_id)R.scene_map.size() - 1;
+    });
+}
+
+pcr_status pcr_router_serve_start(pcr_router* r)
+{
+    return guard([&] {
+        for (pcr::Engine* e : RT(r).eng) e->serve_start();
+    });
+}
+
+pcr_status pcr_router_serve_stop(pcr_router* r)
+{
+    return guard([&] {
+        for (pcr::Engine* e : RT(r).eng) e->serve_stop();
+    });
+}
+
+pcr_status pcr_router_submit(pcr_router* r, pcr_scene_id scene, const pcr_render_desc* desc, int64_t* ticket)
+{
+    return guard([&] {
+        pcr_router& R = RT(r);
+        if (!desc || !ticket) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        std::lock_guard<std::mutex> g(R.mu);
+        if (scene < 0 || scene >= (int)R.scene_map.size()) throw pcr::PcrError(PCR_ERR_NOT_FOUND, "unknown scene");
+        int best = 0;
+        for (int i = 1; i < (int)R.eng.size(); i++)
+            if (R.load[i] < R.load[best]) best = i;
+        const int64_t paths = (int64_t)desc->width * desc->height * desc->samples * std::max(1, desc->aa_samples);
+        const int64_t id = R.eng[best]->submit(R.scene_map[scene][best], *desc);
+        R.load[best] += paths;
+        R.routed[best]++;
+        *ticket = R.next++;
+        R.tickets[*ticket] = {best, id, paths};
+    });
+}
+
+namespace {
+pcr_router::Ticket ticket_of(pcr_router& R, int64_t t)
+{
+    std::lock_guard<std::mutex> g(R.mu);
+    auto it = R.tickets.find(t);
+    if (it == R.tickets.end()) throw pcr::PcrError(PCR_ERR_NOT_FOUND, "unknown ticket");
+    return it->second;
+}
+}  // namespace
+
+pcr_status pcr_router_wait(pcr_router* r, int64_t ticket, int64_t timeout_ms)
+{
+    return guard([&] {
+        pcr_router& R = RT(r);
+        const pcr_router::Ticket t = ticket_of(R, ticket);
+        R.eng[t.ctx]->wait(t.id, timeout_ms);
+    });
+}
+
+pcr_status pcr_router_fetch(pcr_router* r, int64_t ticket, float* hdr_out, uint8_t* rgb8_out,
+                            pcr_render_stats* stats)
+{
+    return guard([&] {
+        pcr_router& R = RT(r);
+        const pcr_router::Ticket t = ticket_of(R, ticket);
+        R.eng[t.ctx]->fetch(t.id, hdr_out, rgb8_out, stats);
+        std::lock_guard<std::mutex> g(R.mu);
+        R.load[t.ctx] -= t.paths;
+        R.tickets.erase(ticket);
+    });
+}
+
+pcr_status pcr_router_load(pcr_router* r, int64_t* outstanding_paths, int64_t* routed)
+{
+    return guard([&] {
+        pcr_router& R = RT(r);
+        std::lock_guard<std::mutex> g(R.mu);
+        for (size_t i = 0; i < R.eng.size(); i++) {
+            if (outstanding_paths) outstanding_paths[i] = R.load[i];
+            if (routed) routed[i] = R.routed[i];
+        }
     });
 }
 

@@ -1,4 +1,5 @@
-"""Served mode (continuous batching) and the autotuner, through the C ABI.
+"""Served mode (continuous batching), the autotuner and the request router,
+through the C ABI.
 
 Serving admits renders on the engine's own thread as request slots and the
 device-memory budget free up; a request that arrives while others are on the
@@ -122,3 +123,38 @@ def test_autotune_picks_from_grid_and_keeps_results():
             assert np.allclose(ctx.fetch(i)[0], b, rtol=RTOL, atol=ATOL)
     finally:
         ctx.close()
+
+
+def test_router_spreads_requests_and_keeps_results():
+    """Two contexts on one GPU stand in for two devices: the router replicates
+    the scenes, sends each request to the context with fewer paths
+    outstanding, and every image equals the same render on one context."""
+    from pcr_b200 import capi
+    a = capi.Context(device=0, queue_capacity=1 << 17)
+    b = capi.Context(device=0, queue_capacity=1 << 17)
+    try:
+        router = capi.Router([a, b])
+        names = ["cornell", "cornell-spheres"]
+        rsid = {v: router.load_scene_json(scene_path(v), GOLDEN) for v in names}
+        sid = {v: a.load_scene_json(scene_path(v), GOLDEN) for v in names}
+        reqs = [(names[k % 2], capi.render_desc(32 + 8 * k, depth=3, samples=2 + k % 3, shadow=2, seed=700 + k))
+                for k in range(10)]
+        want = [a.render(sid[v], d)[0] for v, d in reqs]
+        router.serve_start()
+        tickets = [router.submit(rsid[v], d) for v, d in reqs]
+        got = []
+        for t, (_, d) in zip(tickets, reqs):
+            router.wait(t, 120_000)
+            got.append(router.fetch(t, d.width, d.height)[0])
+        router.serve_stop()
+        for w, g in zip(want, got):
+            assert np.allclose(w, g, rtol=RTOL, atol=ATOL)
+        outstanding, routed = router.load()
+        assert outstanding == [0, 0]
+        assert sum(routed) == len(reqs) and min(routed) >= 3
+        with pytest.raises(capi.PcrError):
+            router.fetch(tickets[0], 32, 32)     # a ticket is fetched once
+        router.close()
+    finally:
+        a.close()
+        b.close()
