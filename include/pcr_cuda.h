@@ -98,6 +98,12 @@ typedef struct {
      * wavefront's default (code/Includes/GpuDefaults.h:44-50); 1 = passes
      * as large as the queue (wavefrontMultiSample) */
     int32_t multi_sample;
+    /* Sample range [sample_begin, sample_end) of `samples` (0, 0 = all).  A
+     * render split across GPUs gives each one a range; the HDR images are
+     * then partial sums (each already divided by samples * aa) that add up
+     * to the full image, and pcr_tonemap makes the 8-bit image of the sum.
+     * Not with adaptive sampling. */
+    int32_t sample_begin, sample_end;
 } pcr_render_desc;
 
 typedef struct {
@@ -234,6 +240,12 @@ pcr_status pcr_trace_closest(pcr_ctx *ctx, pcr_scene_id scene, const float *rays
  * per-ray counts of internal nodes visited and triangles tested (may be NULL). */
 pcr_status pcr_trace_bvh(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, int64_t n,
                          int32_t *tri_id, float *t, int32_t *counts);
+/* Reinhard / ACES tone map and 8-bit quantisation of a linear sRGB image
+ * (code/Renderer.cpp:365-382), with the bilateral denoise when asked; the
+ * last step of a render split across GPUs. */
+pcr_status pcr_tonemap(pcr_ctx *ctx, const float *hdr, int32_t width, int32_t height, int32_t aces, int32_t denoise,
+                       uint8_t *rgb8_out);
+
 /* ------------------------------------------------------------- router
  * Request router over several contexts, typically one per GPU of a node
  * (the scale-out of the serving path; the reference renders on one device

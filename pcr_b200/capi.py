@@ -27,7 +27,7 @@ EXPORTS = [
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
     "pcr_fetch", "pcr_cancel", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
     "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_eval_stage",
-    "pcr_router_create", "pcr_router_destroy", "pcr_router_scene_load_json", "pcr_router_serve_start",
+    "pcr_tonemap", "pcr_router_create", "pcr_router_destroy", "pcr_router_scene_load_json", "pcr_router_serve_start",
     "pcr_router_serve_stop", "pcr_router_submit", "pcr_router_wait", "pcr_router_fetch", "pcr_router_load",
 ]
 
@@ -87,7 +87,9 @@ class RenderDesc(C.Structure):
     _fields_ = [(n, C.c_int32) for n in (
         "width", "height", "depth", "samples", "shadow_samples", "spectral", "hero_samples", "mis", "russian",
         "stratified", "aa_samples", "adaptive", "aces", "denoise")] + [("seed", C.c_uint64), ("priority", C.c_int32),
-                                                                ("multi_sample", C.c_int32)]
+                                                                ("multi_sample", C.c_int32),
+                                                                ("sample_begin", C.c_int32),
+                                                                ("sample_end", C.c_int32)]
 
 
 class RenderStats(C.Structure):
@@ -155,6 +157,7 @@ def load_library():
         "pcr_trace_closest": [P, C.c_int32, fp, C.c_int64, ip, ip, fp],
         "pcr_trace_bvh": [P, C.c_int32, fp, C.c_int64, ip, fp, ip],
         "pcr_trace_shadow": [P, C.c_int32, fp, fp, C.c_int64, ip],
+        "pcr_tonemap": [P, fp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint8)],
         "pcr_router_create": [C.POINTER(P), C.POINTER(P), C.c_int32],
         "pcr_router_destroy": [P],
         "pcr_router_scene_load_json": [P, C.c_char_p, C.c_char_p, C.c_char_p, ip],
@@ -189,10 +192,10 @@ def _ip(a):
 
 def render_desc(width, height=None, depth=4, samples=16, shadow=4, spectral=True, hero=4, mis=False,
                 russian=False, stratified=False, aa=1, adaptive=False, aces=False, denoise=False, seed=1,
-                priority=0, multi_sample=False) -> RenderDesc:
+                priority=0, multi_sample=False, sample_begin=0, sample_end=0) -> RenderDesc:
     return RenderDesc(width, height or width, depth, samples, shadow, int(spectral), hero, int(mis),
                       int(russian), int(stratified), aa, int(adaptive), int(aces), int(denoise), seed, priority,
-                      int(multi_sample))
+                      int(multi_sample), sample_begin, sample_end)
 
 
 class HostScene:
@@ -417,6 +420,14 @@ class Context:
         n = r.shape[0]
         out = np.zeros(n, np.int32)
         _check(self.L.pcr_trace_shadow(self.h, sid, _fp(r), _fp(d2), n, _ip(out)))
+        return out
+
+    def tonemap(self, hdr: np.ndarray, aces=False, denoise=False) -> np.ndarray:
+        """8-bit image of a linear sRGB image (H, W, 3), on the device."""
+        h = np.ascontiguousarray(hdr, np.float32)
+        out = np.zeros(h.shape, np.uint8)
+        _check(self.L.pcr_tonemap(self.h, _fp(h), h.shape[1], h.shape[0], int(aces), int(denoise),
+                                  out.ctypes.data_as(C.POINTER(C.c_uint8))))
         return out
 
     def eval_stage(self, what: int, inp: np.ndarray, params: np.ndarray | None = None) -> np.ndarray:

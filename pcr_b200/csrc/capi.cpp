@@ -294,6 +294,15 @@ pcr_status pcr_trace_bvh(pcr_ctx* ctx, pcr_scene_id scene, const float* rays, in
     });
 }
 
+pcr_status pcr_tonemap(pcr_ctx* ctx, const float* hdr, int32_t width, int32_t height, int32_t aces, int32_t denoise,
+                       uint8_t* rgb8_out)
+{
+    return guard([&] {
+        if (!hdr || !rgb8_out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        E(ctx).tonemap(hdr, width, height, aces, denoise, rgb8_out);
+    });
+}
+
 pcr_status pcr_router_create(pcr_router** out, pcr_ctx* const* ctxs, int32_t n)
 {
     return guard([&] {

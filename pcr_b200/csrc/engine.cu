@@ -631,6 +631,12 @@ void Engine::validate(int scene, const pcr_render_desc& d) const
     if (d.depth > 255) throw PcrError(PCR_ERR_INVALID, "depth above 255");
     if (d.shadow_samples > kMaxShadow) throw PcrError(PCR_ERR_INVALID, "more than 64 shadow samples per hit");
     const int64_t px = (int64_t)d.width * d.height;
+    if (d.sample_end != 0 || d.sample_begin != 0) {
+        if (d.sample_begin < 0 || d.sample_end <= d.sample_begin || d.sample_end > d.samples)
+            throw PcrError(PCR_ERR_INVALID, "sample range must satisfy 0 <= sample_begin < sample_end <= samples");
+        if (d.adaptive && d.aa_samples > 1)
+            throw PcrError(PCR_ERR_INVALID, "a sample range cannot be combined with adaptive sampling");
+    }
     const int64_t ppp = (int64_t)d.samples * std::max(1, d.aa_samples);
     if (px >= (1ll << 31) || ppp >= (1ll << 31) || px * ppp >= (1ll << 62))
         throw PcrError(PCR_ERR_INVALID, "render too large");
@@ -641,6 +647,13 @@ void Engine::validate(int scene, const pcr_render_desc& d) const
 // Adaptive sampling runs only with more than one aa sample per pixel (the
 // convergence test needs 4 rounds; with aa = 1 there is a single round).
 static bool adaptive_rounds(const pcr_render_desc& d) { return d.adaptive && d.aa_samples > 1; }
+
+// The request's samples per aa round: [sample_begin, sample_end) of
+// `samples`, or all of them.
+static int local_spp(const pcr_render_desc& d)
+{
+    return d.sample_end > 0 ? d.sample_end - d.sample_begin : d.samples;
+}
 
 int64_t Engine::request_bytes(const pcr_render_desc& d) const
 {
@@ -686,7 +699,9 @@ void Engine::activate(Request& r, int slot)
     R.depth = d.depth;
     R.aa = std::max(1, d.aa_samples);
     R.spp = d.samples;
-    R.paths_per_pixel = R.aa * R.spp;
+    R.sample0 = d.sample_end > 0 ? d.sample_begin : 0;
+    R.local_spp = local_spp(d);
+    R.paths_per_pixel = R.aa * R.local_spp;
     R.shadow = d.shadow_samples;
     R.flags = (d.spectral ? kReqSpectral : 0) | (d.mis ? kReqMIS : 0) | (d.russian ? kReqRussian : 0) |
               (d.stratified ? kReqStratified : 0);
@@ -1172,7 +1187,7 @@ void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, ui
     activate(r, 0);
     slot_owner_[0] = -1;  // the plain request is not in the request map
     upload_active();
-    const int64_t total = px * desc.samples * std::max(1, desc.aa_samples);
+    const int64_t total = px * local_spp(desc) * std::max(1, desc.aa_samples);
     const int64_t passes = (total + pass - 1) / pass;
     int cur = 0;
     for (int64_t it = 0; it < passes * (int64_t)desc.depth; it++) {
@@ -1278,7 +1293,9 @@ DRequest Engine::make_request(const pcr_render_desc& d, int scene, double* accum
     R.depth = d.depth;
     R.aa = std::max(1, d.aa_samples);
     R.spp = d.samples;
-    R.paths_per_pixel = R.aa * R.spp;
+    R.sample0 = d.sample_end > 0 ? d.sample_begin : 0;
+    R.local_spp = local_spp(d);
+    R.paths_per_pixel = R.aa * R.local_spp;
     R.shadow = d.shadow_samples;
     R.flags = (d.spectral ? kReqSpectral : 0) | (d.mis ? kReqMIS : 0) | (d.russian ? kReqRussian : 0) |
               (d.stratified ? kReqStratified : 0);
@@ -1424,7 +1441,7 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
         CK(cudaGetLastError());
         cur ^= 1;
     };
-    const int64_t total = px * desc.samples * std::max(1, desc.aa_samples);
+    const int64_t total = px * local_spp(desc) * std::max(1, desc.aa_samples);
     const int64_t passes = (total + pass - 1) / pass;
     for (int64_t it = 0; it < passes * (int64_t)desc.depth; it++) iteration();
     for (int extra = 0;; extra++) {
@@ -1522,6 +1539,32 @@ void Engine::trace_shadow(int scene, const float* rays, const float* dist2, int6
     CK(cudaFreeAsync(d_rays, stream_));
     CK(cudaFreeAsync(d_d2, stream_));
     CK(cudaFreeAsync(d_b, stream_));
+    CK(cudaStreamSynchronize(stream_));
+}
+
+void Engine::tonemap(const float* hdr, int width, int height, int aces_tm, int denoise, uint8_t* rgb8)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    if (width <= 0 || height <= 0) throw PcrError(PCR_ERR_INVALID, "width and height must be positive");
+    const int64_t px = (int64_t)width * height;
+    float* d_hdr = nullptr;
+    unsigned char *d_rgb = nullptr, *d_tmp = nullptr;
+    CK(cudaMallocFromPoolAsync(&d_hdr, px * 3 * sizeof(float), pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&d_rgb, px * 3, pool_, stream_));
+    CK(cudaMemcpyAsync(d_hdr, hdr, px * 3 * sizeof(float), cudaMemcpyHostToDevice, stream_));
+    const int grid = (int)std::max<int64_t>(1, std::min<int64_t>((px + 255) / 256, (int64_t)sms_ * 8));
+    k_tonemap<<<grid, 256, 0, stream_>>>(d_hdr, (int)px, aces_tm, d_rgb);
+    if (denoise) {
+        CK(cudaMallocFromPoolAsync(&d_tmp, px * 3, pool_, stream_));
+        k_bilateral<<<grid, 256, 0, stream_>>>(d_rgb, d_tmp, width, height);
+        k_bilateral<<<grid, 256, 0, stream_>>>(d_tmp, d_rgb, width, height);
+    }
+    CK(cudaGetLastError());
+    CK(cudaMemcpyAsync(rgb8, d_rgb, px * 3, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaFreeAsync(d_hdr, stream_));
+    CK(cudaFreeAsync(d_rgb, stream_));
+    if (d_tmp) CK(cudaFreeAsync(d_tmp, stream_));
     CK(cudaStreamSynchronize(stream_));
 }
 

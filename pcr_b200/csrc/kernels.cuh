@@ -249,7 +249,8 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
             sample = (uint32_t)(R.round * R.spp + (int)(q % R.spp));
         } else {
             pixel = (uint32_t)(path / R.paths_per_pixel);
-            sample = (uint32_t)(path % R.paths_per_pixel);
+            const int q = (int)(path % R.paths_per_pixel);  // local sample
+            sample = (uint32_t)((q / R.local_spp) * R.spp + R.sample0 + q % R.local_spp);
         }
         const int px = (int)(pixel % (uint32_t)R.width), py = (int)(pixel / (uint32_t)R.width);
         float jx = 0.f, jy = 0.f;
@@ -919,6 +920,19 @@ __global__ void k_resolve(const double* __restrict__ acc, int npix, double inv_n
             rgb8[i * 3 + 1] = quantize(m.y);
             rgb8[i * 3 + 2] = quantize(m.z);
         }
+    }
+}
+
+// Tone map + quantise a linear sRGB image (the last step of k_resolve).
+__global__ void k_tonemap(const float* __restrict__ hdr, int npix, int aces_tm, unsigned char* __restrict__ rgb8)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < npix; i += gridDim.x * blockDim.x) {
+        const float3 c = make_float3(hdr[i * 3], hdr[i * 3 + 1], hdr[i * 3 + 2]);
+        const float3 m = aces_tm ? make_float3(aces(c.x), aces(c.y), aces(c.z))
+                                 : make_float3(reinhard(c.x), reinhard(c.y), reinhard(c.z));
+        rgb8[i * 3] = quantize(m.x);
+        rgb8[i * 3 + 1] = quantize(m.y);
+        rgb8[i * 3 + 2] = quantize(m.z);
     }
 }
 

@@ -129,7 +129,9 @@ struct DRequest {
     float4* welford;
     long long round_base;     // paths issued before this round
     int round;
-    int pad_;
+    // sample range [sample0, sample0 + local_spp) of each aa round (a render
+    // split across GPUs); paths_per_pixel = local_spp * aa
+    int sample0, local_spp;
 };
 
 // Path state, structure of arrays, one entry per queued path.

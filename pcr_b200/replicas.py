@@ -59,8 +59,47 @@ class Replicas:
         self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
         return float(t.item())
 
+    def sum_array(self, a):
+        """Element-wise sum of a numpy array over the ranks (all ranks get it)."""
+        import numpy as np
+        if not self.dist:
+            return np.asarray(a)
+        import torch
+        dev = f"cuda:{self.local}" if self.backend == "nccl" else "cpu"
+        t = torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+        self.dist.all_reduce(t, op=self.dist.ReduceOp.SUM)
+        return t.cpu().numpy()
+
     def close(self) -> None:
         if self.dist:
             self.dist.barrier()
             self.dist.destroy_process_group()
             self.dist = None
+
+
+def sample_range(spp: int, rank: int, world: int):
+    """Rank's contiguous share [begin, end) of the samples 0..spp-1."""
+    base, extra = divmod(spp, world)
+    begin = rank * base + min(rank, extra)
+    return begin, begin + base + (1 if rank < extra else 0)
+
+
+def split_render(ctx, sid: int, desc, rep: Replicas):
+    """One render split across the replicas by sample range (the multi-GPU
+    single render): every path's random numbers depend on its pixel and
+    sample number only, so each rank traces its own samples of every aa
+    round; the partial HDR images (each divided by the full samples * aa)
+    are summed by an all-reduce and tone-mapped on the device.  Returns
+    (hdr, rgb8) on every rank."""
+    import copy
+
+    import numpy as np
+    b, e = sample_range(desc.samples, rep.rank, rep.world)
+    if e > b:
+        d = copy.copy(desc)
+        d.sample_begin, d.sample_end = b, e
+        part = ctx.render(sid, d, want_rgb=False)[0]
+    else:
+        part = np.zeros((desc.height, desc.width, 3), np.float32)
+    hdr = rep.sum_array(part).astype(np.float32)
+    return hdr, ctx.tonemap(hdr, aces=bool(desc.aces), denoise=bool(desc.denoise))

@@ -144,3 +144,32 @@ def test_mesh_scene_mean_matches_oracle(ctx, O, glass):
     tol = 0.04 if glass else 0.03
     assert np.all(np.abs(mg - mo) <= tol * np.abs(mo) + 1e-3), (mg, mo)
     ctx.release_scene(sid)
+
+
+def test_sample_range_partials_sum_to_the_full_render(ctx):
+    """A render split by sample range (the multi-GPU single render, here two
+    ranges on one GPU): the partial HDR images add up to the full render and
+    the device tone map of the sum gives its 8-bit image."""
+    from pcr_b200 import capi
+    from pcr_b200.replicas import sample_range
+    sid = ctx.load_scene_json(scene_path("cornell-glass"), GOLDEN)
+    for aa, stratified in ((1, False), (3, False), (1, True)):
+        full = capi.render_desc(40, 36, depth=4, samples=9, shadow=2, aa=aa, stratified=stratified, seed=81)
+        hdr, rgb, st = ctx.render(sid, full)
+        acc = np.zeros_like(hdr, dtype=np.float64)
+        paths = 0
+        for rank in range(3):
+            b, e = sample_range(9, rank, 3)
+            part = capi.render_desc(40, 36, depth=4, samples=9, shadow=2, aa=aa, stratified=stratified, seed=81,
+                                    sample_begin=b, sample_end=e)
+            h, _, s = ctx.render(sid, part, want_rgb=False)
+            acc += h
+            paths += s.paths
+        assert paths == st.paths
+        assert np.allclose(acc, hdr, rtol=1e-5, atol=1e-6)
+        rgb2 = ctx.tonemap(acc.astype(np.float32))
+        d = np.abs(rgb2.astype(int) - rgb.astype(int))
+        assert d.max() <= 1 and (d > 0).mean() < 1e-3
+    with pytest.raises(capi.PcrError):
+        ctx.render(sid, capi.render_desc(16, samples=4, sample_begin=3, sample_end=2))
+    ctx.release_scene(sid)

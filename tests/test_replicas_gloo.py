@@ -63,3 +63,52 @@ def test_single_process_needs_no_process_group():
     assert rep.world == 1 and rep.dist is None
     assert rep.max(3.5) == 3.5 and rep.sum(2.0) == 2.0 and rep.seed(7) == 7
     rep.close()
+
+
+class _FakeCtx:
+    """Stands in for a GPU context: a 'render' of a sample range returns the
+    range's sample count in every pixel (what a partial sum contributes)."""
+
+    def render(self, sid, d, want_rgb=True):
+        import numpy as np
+        return np.full((d.height, d.width, 3), float(d.sample_end - d.sample_begin), np.float32), None, None
+
+    def tonemap(self, hdr, aces=False, denoise=False):
+        return (hdr * 0).astype("uint8") + 7
+
+
+def _split_main(rank, world, port, q):
+    os.environ.update({"MASTER_ADDR": "127.0.0.1", "MASTER_PORT": str(port), "RANK": str(rank),
+                       "WORLD_SIZE": str(world), "LOCAL_RANK": str(rank)})
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    from pcr_b200 import capi
+    from pcr_b200.replicas import Replicas, sample_range, split_render
+    rep = Replicas("gloo", timeout_s=60)
+    desc = capi.render_desc(6, 4, samples=7)
+    hdr, rgb = split_render(_FakeCtx(), 0, desc, rep)
+    q.put({"rank": rank, "range": sample_range(7, rank, world), "hdr": float(hdr.mean()), "rgb": int(rgb.max())})
+    rep.close()
+
+
+def test_split_render_ranges_cover_samples_and_sum():
+    from pcr_b200.replicas import sample_range
+    for spp in (1, 2, 7, 64):
+        for world in (1, 2, 3, 8):
+            r = [sample_range(spp, k, world) for k in range(world)]
+            assert r[0][0] == 0 and r[-1][1] == spp
+            assert all(r[k][1] == r[k + 1][0] for k in range(world - 1))
+            assert max(e - b for b, e in r) - min(e - b for b, e in r) <= 1
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_split_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted([q.get(timeout=120) for _ in procs], key=lambda r: r["rank"])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert [r["range"] for r in res] == [(0, 4), (4, 7)]
+    assert all(r["hdr"] == 7.0 for r in res)      # the partial sums add up to all 7 samples
+    assert all(r["rgb"] == 7 for r in res)
