@@ -640,8 +640,8 @@ void Engine::validate(int scene, const pcr_render_desc& d) const
     const int64_t ppp = (int64_t)d.samples * std::max(1, d.aa_samples);
     if (px >= (1ll << 31) || ppp >= (1ll << 31) || px * ppp >= (1ll << 62))
         throw PcrError(PCR_ERR_INVALID, "render too large");
-    if (d.shadow_samples > 8 && (int64_t)tune_.queue_capacity * 4 * d.shadow_samples > (int64_t)shadow_cap_)
-        throw PcrError(PCR_ERR_INVALID, "shadow samples exceed the shadow queue sizing");
+    if ((int64_t)queue_cap_ * d.shadow_samples >= (1ll << 31))
+        throw PcrError(PCR_ERR_INVALID, "shadow samples x queue capacity above 2^31 shadow records");
 }
 
 // Adaptive sampling runs only with more than one aa sample per pixel (the
@@ -662,9 +662,35 @@ int64_t Engine::request_bytes(const pcr_render_desc& d) const
     return px * 3 * (8 + 4 + 1) + (adaptive_rounds(d) ? px * (32 + 8) : 0);
 }
 
+// The shadow queue holds shadow_samples records for every path slot of a
+// launch (8 by default).  A request with more shadow samples grows it
+// between iterations: shadow records never outlive the iteration that
+// writes them, so the buffer can be replaced once the stream is drained.
+// The caller holds run_mu_.
+void Engine::ensure_shadow_capacity(int shadow_samples)
+{
+    const int64_t need = (int64_t)queue_cap_ * std::max(8, shadow_samples);
+    if (need <= shadow_cap_) return;
+    CK(cudaStreamSynchronize(stream_));
+    for (float4* p : {sq_.o, sq_.d, sq_.c}) {
+        auto it = std::find(qallocs_.begin(), qallocs_.end(), (void*)p);
+        if (it != qallocs_.end()) qallocs_.erase(it);
+        CK(cudaFree(p));
+    }
+    shadow_cap_ = (int)need;
+    sq_.o = dalloc<float4>(shadow_cap_, qallocs_);
+    sq_.d = dalloc<float4>(shadow_cap_, qallocs_);
+    sq_.c = dalloc<float4>(shadow_cap_, qallocs_);
+    graph_dirty_ = true;
+}
+
 int64_t Engine::submit(int scene, const pcr_render_desc& desc)
 {
     validate(scene, desc);
+    if ((int64_t)queue_cap_ * desc.shadow_samples > shadow_cap_) {
+        std::lock_guard<std::mutex> g(run_mu_);
+        ensure_shadow_capacity(desc.shadow_samples);
+    }
     auto r = std::make_unique<Request>();
     r->scene = scene;
     r->desc = desc;
@@ -1170,6 +1196,7 @@ void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, ui
     CK(cudaSetDevice(device_));
     validate(scene, desc);
     if (!active_slots_.empty() || serving_) throw PcrError(PCR_ERR_INVALID, "plain render while batched work is active");
+    ensure_shadow_capacity(desc.shadow_samples);
     auto t0 = std::chrono::steady_clock::now();
     Request r;
     r.id = -1;

@@ -103,6 +103,7 @@ public:
     cudaStream_t stream() const { return stream_; }
 
 private:
+    void ensure_shadow_capacity(int shadow_samples);
     void alloc_buffers();
     void free_buffers();
     void validate(int scene, const pcr_render_desc& d) const;

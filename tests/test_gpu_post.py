@@ -173,3 +173,24 @@ def test_sample_range_partials_sum_to_the_full_render(ctx):
     with pytest.raises(capi.PcrError):
         ctx.render(sid, capi.render_desc(16, samples=4, sample_begin=3, sample_end=2))
     ctx.release_scene(sid)
+
+
+def test_many_shadow_samples_grow_the_shadow_queue(ctx):
+    """More than 8 shadow samples per hit (the reference takes any S): the
+    shadow queue grows between iterations.  The estimate has the same
+    expectation as with few samples, and the batched render equals the
+    plain one."""
+    from pcr_b200 import capi
+    sid = ctx.load_scene_json(scene_path("cornell"), GOLDEN)
+    few = ctx.render(sid, capi.render_desc(48, depth=3, samples=64, shadow=2, seed=91))[0]
+    many_d = capi.render_desc(48, depth=3, samples=64, shadow=40, seed=91)
+    many, _, st = ctx.render(sid, many_d)
+    assert st.paths == 48 * 48 * 64
+    mf, mm = few.reshape(-1, 3).mean(0), many.reshape(-1, 3).mean(0)
+    assert np.all(np.abs(mm - mf) <= 0.03 * np.abs(mf)), (mm, mf)
+    rid = ctx.submit(sid, many_d)
+    ctx.run_until_idle()
+    assert np.allclose(ctx.fetch(rid)[0], many, rtol=1e-6, atol=1e-7)
+    with pytest.raises(capi.PcrError):
+        ctx.render(sid, capi.render_desc(16, samples=1, shadow=65))
+    ctx.release_scene(sid)
