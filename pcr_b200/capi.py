@@ -361,13 +361,23 @@ class Context:
     def wait(self, rid: int, timeout_ms: int = -1) -> None:
         _check(self.L.pcr_wait(self.h, rid, timeout_ms))
 
-    def fetch(self, rid: int, want_hdr=True, want_rgb=True):
-        w, h = self._keep.pop(rid)
-        hdr = np.zeros((h, w, 3), np.float32) if want_hdr else None
-        rgb = np.zeros((h, w, 3), np.uint8) if want_rgb else None
+    def fetch(self, rid: int, want_hdr=True, want_rgb=True, hdr_out=None, rgb_out=None):
+        """Copies a finished request's images to the host: new arrays, or the
+        caller's (H, W, 3) float32 / uint8 buffers when given."""
+        w, h = self._keep[rid]
+        hdr = rgb = None
+        if want_hdr:
+            hdr = hdr_out if hdr_out is not None else np.zeros((h, w, 3), np.float32)
+            if hdr.shape != (h, w, 3) or hdr.dtype != np.float32 or not hdr.flags.c_contiguous:
+                raise ValueError("hdr_out must be a C-contiguous float32 (H, W, 3) array")
+        if want_rgb:
+            rgb = rgb_out if rgb_out is not None else np.zeros((h, w, 3), np.uint8)
+            if rgb.shape != (h, w, 3) or rgb.dtype != np.uint8 or not rgb.flags.c_contiguous:
+                raise ValueError("rgb_out must be a C-contiguous uint8 (H, W, 3) array")
         st = RenderStats()
         _check(self.L.pcr_fetch(self.h, rid, _fp(hdr) if want_hdr else None,
                                 rgb.ctypes.data_as(C.POINTER(C.c_uint8)) if want_rgb else None, C.byref(st)))
+        del self._keep[rid]
         return hdr, rgb, st
 
     def cancel(self, rid: int) -> None:
