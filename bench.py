@@ -65,7 +65,7 @@ def args_():
     p.add_argument("--queue", type=int, default=0, help="paths in flight (0: library default)")
     p.add_argument("--no-autotune", action="store_true",
                    help="skip the autotuner (queue size, block size, issue chunk, refill cadence)")
-    p.add_argument("--serve-requests", type=int, default=400)
+    p.add_argument("--serve-requests", type=int, default=2000, help="served stream length (2000: the serving config)")
     p.add_argument("--serve-rate", type=float, default=200.0)
     return p.parse_args()
 
@@ -317,6 +317,7 @@ def serve_run(ctx, sids, files, data, a):
     return {"requests": len(ids), "rate_req_s": a.serve_rate, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
             "paths_per_s": paths / (t_last / 1e3), "span_s": t_last / 1e3,
+            "offered_paths_per_s": paths / max(reqs[-1]["arrival"], 1e-9),
             "mesh_fraction": 0.2, "resolution": "log-uniform 64..1024"}
 
 
