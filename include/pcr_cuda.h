@@ -93,7 +93,8 @@ typedef struct {
      * (code/Denoise.cpp:14-86). */
     int32_t aa_samples, adaptive, aces, denoise;
     uint64_t seed;           /* 0 -> 1 */
-    int32_t priority;        /* serving: lower runs first among equals (0 default) */
+    int32_t priority;        /* batched / served: pending requests are admitted lowest value
+                              * first, in submit order among equals (0 default) */
     /* plain method only: 0 = one sample per pixel per pass, the reference
      * wavefront's default (code/Includes/GpuDefaults.h:44-50); 1 = passes
      * as large as the queue (wavefrontMultiSample) */

@@ -702,8 +702,16 @@ int64_t Engine::submit(int scene, const pcr_render_desc& desc)
         std::lock_guard<std::mutex> g(mu_);
         id = next_id_++;
         r->id = id;
+        const int prio = desc.priority;
         reqs_[id] = std::move(r);
-        pending_.push_back(id);
+        // admission order: lower priority value first, submit order among equals
+        auto at = pending_.end();
+        while (at != pending_.begin()) {
+            auto prev = std::prev(at);
+            if (reqs_[*prev]->desc.priority <= prio) break;
+            at = prev;
+        }
+        pending_.insert(at, id);
     }
     cv_.notify_all();
     return id;

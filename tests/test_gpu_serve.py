@@ -158,3 +158,24 @@ def test_router_spreads_requests_and_keeps_results():
     finally:
         a.close()
         b.close()
+
+
+def test_pending_requests_are_admitted_by_priority():
+    """A memory budget that holds one request at a time: after the first,
+    pending requests are admitted lowest priority value first, in submit
+    order among equals."""
+    from pcr_b200 import capi
+    ctx = capi.Context(device=0, queue_capacity=1 << 17, memory_budget=128 * 128 * 3 * 13)
+    try:
+        sid = ctx.load_scene_json(scene_path("cornell"), GOLDEN)
+
+        def d(prio, seed):
+            return capi.render_desc(128, depth=2, samples=2, shadow=1, seed=seed, priority=prio)
+        ids = {"a": ctx.submit(sid, d(0, 1)), "b": ctx.submit(sid, d(5, 2)), "c": ctx.submit(sid, d(1, 3)),
+               "e": ctx.submit(sid, d(1, 4)), "f": ctx.submit(sid, d(-2, 5))}
+        ctx.run_until_idle()
+        q = {k: ctx.fetch(i, want_hdr=False, want_rgb=False)[2].queue_ms for k, i in ids.items()}
+        # nothing was admitted before run_until_idle: f (-2), a (0), c (1), e (1), b (5)
+        assert q["f"] < q["a"] < q["c"] < q["e"] < q["b"], q
+    finally:
+        ctx.close()
