@@ -282,7 +282,7 @@ def matched_run(ctx, sids, stream, a, with_cpu):
 
 
 # ------------------------------------------------------------------ served stream
-def serve_run(ctx, sids, files, data, a):
+def serve_run(ctx, sids, files, data, a, n=None, rate=None, seed_off=17):
     """Requests arrive by a Poisson process at `rate` req/s (scene drawn from
     the 10 variants, 20 % the seeded ~70k-triangle mesh scene, glass or
     Lambertian by seed; square resolution log-uniform 64..1024, depth 2..8,
@@ -293,7 +293,9 @@ def serve_run(ctx, sids, files, data, a):
     from pcr_b200 import capi, workloads
     mesh = {False: ctx.load_scene_json(workloads.mesh_scene(59, 11, glass=False), data),
             True: ctx.load_scene_json(workloads.mesh_scene(59, 12, glass=True), data)}
-    reqs = workloads.request_stream(a.serve_requests, a.serve_rate, seed=a.seed + 17)
+    n = n or a.serve_requests
+    rate = rate or a.serve_rate
+    reqs = workloads.request_stream(n, rate, seed=a.seed + seed_off)
     ctx.serve_start()
     t0 = time.perf_counter()
     ids = []
@@ -314,7 +316,7 @@ def serve_run(ctx, sids, files, data, a):
         t_last = max(t_last, r["arrival"] * 1e3 + st.latency_ms)
     ctx.serve_stop()
     lat = np.asarray(lat)
-    return {"requests": len(ids), "rate_req_s": a.serve_rate, "p50_ms": float(np.percentile(lat, 50)),
+    return {"requests": len(ids), "rate_req_s": rate, "p50_ms": float(np.percentile(lat, 50)),
             "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()),
             "paths_per_s": paths / (t_last / 1e3), "span_s": t_last / 1e3,
             "offered_paths_per_s": paths / max(reqs[-1]["arrival"], 1e-9),
@@ -465,6 +467,12 @@ def main():
     serve = None
     if a.serve_requests > 0:
         serve = serve_run(ctx, sids, files, data, a)
+        # the configured 200 req/s exceeds what one GPU serves, so latency
+        # there is mostly backlog; a second stream arrives at 80 % of the
+        # measured service rate (requests served per second above)
+        cap = serve["requests"] / serve["span_s"]
+        serve["at_80pct_capacity"] = serve_run(ctx, sids, files, data, a, n=min(400, a.serve_requests),
+                                               rate=0.8 * cap, seed_off=29)
 
     # ---- Cornell configuration at matched image error
     matched = None
