@@ -212,6 +212,9 @@ pcr_status pcr_wait(pcr_ctx *ctx, pcr_request_id id, int64_t timeout_ms);
 /* Copies the finished result out and frees the request's device memory. */
 pcr_status pcr_fetch(pcr_ctx *ctx, pcr_request_id id, float *hdr_out, uint8_t *rgb8_out,
                      pcr_render_stats *stats);
+/* Cancels a request still waiting for admission (PCR_ERR_INVALID once it
+ * runs).  pcr_wait on it then returns PCR_ERR_CANCELLED; pcr_fetch returns
+ * PCR_ERR_CANCELLED and releases it. */
 pcr_status pcr_cancel(pcr_ctx *ctx, pcr_request_id id);
 
 /* ------------------------------------------------------------- engine info */

@@ -375,8 +375,13 @@ class Context:
             if rgb.shape != (h, w, 3) or rgb.dtype != np.uint8 or not rgb.flags.c_contiguous:
                 raise ValueError("rgb_out must be a C-contiguous uint8 (H, W, 3) array")
         st = RenderStats()
-        _check(self.L.pcr_fetch(self.h, rid, _fp(hdr) if want_hdr else None,
-                                rgb.ctypes.data_as(C.POINTER(C.c_uint8)) if want_rgb else None, C.byref(st)))
+        try:
+            _check(self.L.pcr_fetch(self.h, rid, _fp(hdr) if want_hdr else None,
+                                    rgb.ctypes.data_as(C.POINTER(C.c_uint8)) if want_rgb else None, C.byref(st)))
+        except PcrError as e:
+            if e.status == 7:      # cancelled: the library released it
+                del self._keep[rid]
+            raise
         del self._keep[rid]
         return hdr, rgb, st
 

@@ -1151,6 +1151,15 @@ void Engine::wait(int64_t id, int64_t timeout_ms)
 
 void Engine::fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st)
 {
+    {
+        // a cancelled request is released by its fetch, which reports it
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = reqs_.find(id);
+        if (it != reqs_.end() && it->second->state == ReqState::Cancelled) {
+            reqs_.erase(it);
+            throw PcrError(PCR_ERR_CANCELLED, "request cancelled");
+        }
+    }
     if (!poll(id)) throw PcrError(PCR_ERR_INVALID, "request not finished");
     std::unique_ptr<Request> owned;
     {

@@ -90,6 +90,12 @@ def test_cancel_pending_request():
         with pytest.raises(capi.PcrError) as e:
             ctx.wait(r2, 60_000)
         assert e.value.status == 7
+        with pytest.raises(capi.PcrError) as e:       # fetch reports it and releases it
+            ctx.fetch(r2)
+        assert e.value.status == 7
+        with pytest.raises(capi.PcrError) as e:
+            ctx.poll(r2)
+        assert e.value.status == 4                    # gone
         ctx.wait(r0, 60_000)
         ctx.wait(r1, 60_000)
         ctx.fetch(r0, want_hdr=False, want_rgb=False)
