@@ -15,6 +15,8 @@
 #include <memory>
 #include <sstream>
 #include <stdexcept>
+#include <future>
+#include <thread>
 
 #include "engine.h"
 
@@ -536,10 +538,35 @@ struct Box {
 inline float centroid(const pcr_triangle& t, int a) { return (t.v0[a] + t.v1[a] + t.v2[a]) * (1.f / 3.f); }
 inline int bin_of(float c, float lo, float scale) { return std::clamp((int)((c - lo) * scale), 0, 15); }
 
+// Runs fn(chunk, lo, hi) over [begin, end) split into `parts` ordered chunks
+// on parallel threads.
+template <typename F>
+void parallel_chunks(int begin, int end, int parts, F&& fn)
+{
+    std::vector<std::thread> th;
+    const int n = end - begin;
+    for (int k = 0; k < parts; k++) {
+        const int lo = begin + (int)((int64_t)n * k / parts), hi = begin + (int)((int64_t)n * (k + 1) / parts);
+        th.emplace_back([&fn, k, lo, hi] { fn(k, lo, hi); });
+    }
+    for (auto& t : th) t.join();
+}
+
+// The reference's recursive binned-SAH build (code/Bvh/Bvh.cpp:122-325).
+// Large ranges are processed by several host threads with the same result
+// as the sequential build: boxes and bin boxes are merged by min / max and
+// counts by addition, with chunks merged in range order (so even the choice
+// among equal signed zeros matches); sibling subtrees of large nodes are
+// built concurrently into their own node lists and spliced in depth-first
+// order (parent, left subtree, right subtree) with their indices shifted.
+// The two-cursor partition stays sequential per node.
+constexpr int kParallelRange = 1 << 16;   // triangles for chunked passes / concurrent children
+
 struct Builder {
     std::vector<pcr_triangle>& tris;
     std::vector<int32_t>* ids;
     std::vector<pcr_bvh_node>& nodes;
+    int threads;   // threads this builder may use
 
     void swap_tri(int a, int b)
     {
@@ -551,10 +578,21 @@ struct Builder {
     {
         int idx = (int)nodes.size();
         nodes.emplace_back();
-        Box box;
-        for (int i = begin; i < end; i++) box.tri(tris[i]);
-        for (int i = 0; i < 3; i++) { nodes[idx].bmin[i] = box.mn[i]; nodes[idx].bmax[i] = box.mx[i]; }
         const int count = end - begin;
+        const int parts = (count >= kParallelRange && threads > 1) ? threads : 1;
+        Box box, cb;
+        {
+            std::vector<Box> pb(parts), pc(parts);
+            parallel_or_inline(begin, end, parts, [&](int k, int lo, int hi) {
+                for (int i = lo; i < hi; i++) {
+                    pb[k].tri(tris[i]);
+                    float c[3] = {centroid(tris[i], 0), centroid(tris[i], 1), centroid(tris[i], 2)};
+                    pc[k].vert(c);
+                }
+            });
+            for (int k = 0; k < parts; k++) { box.merge(pb[k]); cb.merge(pc[k]); }
+        }
+        for (int i = 0; i < 3; i++) { nodes[idx].bmin[i] = box.mn[i]; nodes[idx].bmax[i] = box.mx[i]; }
         auto leaf = [&] {
             nodes[idx].left_or_first = begin;
             nodes[idx].right_child = 0;
@@ -562,11 +600,6 @@ struct Builder {
             return idx;
         };
         if (count <= 4) return leaf();
-        Box cb;
-        for (int i = begin; i < end; i++) {
-            float c[3] = {centroid(tris[i], 0), centroid(tris[i], 1), centroid(tris[i], 2)};
-            cb.vert(c);
-        }
         int best_axis = -1, best_bin = -1;
         float best_cost = FLT_MAX;
         const float parent = box.area();
@@ -575,13 +608,20 @@ struct Builder {
                 float lo = cb.mn[axis], hi = cb.mx[axis], ext = hi - lo;
                 if (ext < 1e-6f) continue;
                 float scale = (float)16 / ext;
+                std::vector<std::array<Box, 16>> pbins(parts);
+                std::vector<std::array<int, 16>> pcnt(parts);
+                for (auto& c : pcnt) c.fill(0);
+                parallel_or_inline(begin, end, parts, [&](int k, int lo_i, int hi_i) {
+                    for (int i = lo_i; i < hi_i; i++) {
+                        int b = bin_of(centroid(tris[i], axis), lo, scale);
+                        pbins[k][b].tri(tris[i]);
+                        pcnt[k][b]++;
+                    }
+                });
                 Box bins[16];
                 int cnt[16] = {0};
-                for (int i = begin; i < end; i++) {
-                    int b = bin_of(centroid(tris[i], axis), lo, scale);
-                    bins[b].tri(tris[i]);
-                    cnt[b]++;
-                }
+                for (int k = 0; k < parts; k++)
+                    for (int b = 0; b < 16; b++) { bins[b].merge(pbins[k][b]); cnt[b] += pcnt[k][b]; }
                 float lSA[15], rSA[15];
                 int lC[15], rC[15];
                 Box acc;
@@ -620,12 +660,42 @@ struct Builder {
     done:
         const int mid = first;
         if (mid == begin || mid == end) return leaf();
-        int l = rec(begin, mid);
-        int r = rec(mid, end);
+        int l, r;
+        if (threads > 1 && mid - begin >= kParallelRange / 2 && end - mid >= kParallelRange / 2) {
+            // the two subtrees on their own threads, spliced depth-first
+            std::vector<pcr_bvh_node> ln, rn;
+            const int tl = std::max(1, threads / 2), tr = std::max(1, threads - tl);
+            auto fut = std::async(std::launch::async, [&] {
+                Builder sub{tris, ids, ln, tl};
+                sub.rec(begin, mid);
+            });
+            Builder sub{tris, ids, rn, tr};
+            sub.rec(mid, end);
+            fut.get();
+            const int bl = (int)nodes.size(), br = bl + (int)ln.size();
+            for (auto& n : ln)
+                if (n.count == 0) { n.left_or_first += bl; n.right_child += bl; }
+            for (auto& n : rn)
+                if (n.count == 0) { n.left_or_first += br; n.right_child += br; }
+            nodes.insert(nodes.end(), ln.begin(), ln.end());
+            nodes.insert(nodes.end(), rn.begin(), rn.end());
+            l = bl;
+            r = br;
+        } else {
+            l = rec(begin, mid);
+            r = rec(mid, end);
+        }
         nodes[idx].left_or_first = l;
         nodes[idx].right_child = r;
         nodes[idx].count = 0;
         return idx;
+    }
+
+    template <typename F>
+    void parallel_or_inline(int begin, int end, int parts, F&& fn)
+    {
+        if (parts <= 1) fn(0, begin, end);
+        else parallel_chunks(begin, end, parts, fn);
     }
 };
 }  // namespace
@@ -635,7 +705,8 @@ std::vector<pcr_bvh_node> build_bvh(std::vector<pcr_triangle>& tris, std::vector
     std::vector<pcr_bvh_node> nodes;
     if (tris.empty()) return nodes;
     nodes.reserve(2 * tris.size());
-    Builder b{tris, ids, nodes};
+    const int threads = std::max(1, std::min(16, (int)std::thread::hardware_concurrency()));
+    Builder b{tris, ids, nodes, threads};
     b.rec(0, (int)tris.size());
     return nodes;
 }
