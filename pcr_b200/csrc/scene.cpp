@@ -10,6 +10,7 @@
 #include <functional>
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 #include <fstream>
 #include <map>
 #include <memory>
@@ -812,35 +813,50 @@ struct ObjData {
     std::vector<std::array<int, 6>> faces;  // v0 v1 v2 n0 n1 n2 (n = -1 when absent)
 };
 
+// Wavefront OBJ subset the reference's loader reads (v, vn, f with v,
+// v/t, v//n, v/t/n tokens, fans of polygons).  The whole file is read at
+// once and scanned in place; numbers go through strtod / strtol, as before.
 ObjData load_obj(const std::string& path)
 {
-    std::ifstream in(path);
+    std::ifstream in(path, std::ios::binary | std::ios::ate);
     if (!in) throw PcrError(PCR_ERR_SCENE, "Mesh file not found: " + path);
+    const std::streamsize size = in.tellg();
+    in.seekg(0);
+    std::string buf((size_t)std::max<std::streamsize>(size, 0), '\0');
+    if (size > 0 && !in.read(&buf[0], size)) throw PcrError(PCR_ERR_SCENE, "Failed to read OBJ " + path);
+    buf.push_back('\n');
     ObjData d;
-    std::string line;
-    while (std::getline(in, line)) {
-        if (line.size() < 2) continue;
-        if (line[0] == 'v' && line[1] == ' ') {
-            const char* p = line.c_str() + 2;
+    const char* p = buf.c_str();
+    const char* const end = p + buf.size();
+    std::vector<std::pair<int, int>> idx;
+    while (p < end) {
+        const char* eol = static_cast<const char*>(std::memchr(p, '\n', (size_t)(end - p)));
+        if (!eol) eol = end;
+        const size_t len = (size_t)(eol - p);
+        if (len >= 2 && p[0] == 'v' && p[1] == ' ') {
+            const char* q = p + 2;
             char* e;
-            for (int k = 0; k < 3; k++) { d.v.push_back((float)std::strtod(p, &e)); p = e; }
-        } else if (line[0] == 'v' && line[1] == 'n' && line.size() > 2 && line[2] == ' ') {
-            const char* p = line.c_str() + 3;
+            for (int k = 0; k < 3; k++) { d.v.push_back((float)std::strtod(q, &e)); q = e; }
+        } else if (len >= 3 && p[0] == 'v' && p[1] == 'n' && p[2] == ' ') {
+            const char* q = p + 3;
             char* e;
-            for (int k = 0; k < 3; k++) { d.vn.push_back((float)std::strtod(p, &e)); p = e; }
-        } else if (line[0] == 'f' && line[1] == ' ') {
-            std::istringstream is(line.substr(2));
-            std::string tok;
-            std::vector<std::pair<int, int>> idx;
-            while (is >> tok) {
-                int vi = 0, ni = 0;
-                size_t s1 = tok.find('/');
-                vi = std::atoi(tok.substr(0, s1).c_str());
+            for (int k = 0; k < 3; k++) { d.vn.push_back((float)std::strtod(q, &e)); q = e; }
+        } else if (len >= 2 && p[0] == 'f' && p[1] == ' ') {
+            idx.clear();
+            const char* q = p + 2;
+            const int nv = (int)d.v.size() / 3, nn = (int)d.vn.size() / 3;
+            while (q < eol) {
+                while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) q++;
+                if (q >= eol) break;
+                const char* t0 = q;   // one token: v, v/t, v//n or v/t/n
+                while (q < eol && *q != ' ' && *q != '\t' && *q != '\r') q++;
+                const std::string tok(t0, (size_t)(q - t0));
+                int vi = std::atoi(tok.c_str()), ni = 0;
+                const size_t s1 = tok.find('/');
                 if (s1 != std::string::npos) {
-                    size_t s2 = tok.find('/', s1 + 1);
-                    if (s2 != std::string::npos && s2 + 1 < tok.size()) ni = std::atoi(tok.substr(s2 + 1).c_str());
+                    const size_t s2 = tok.find('/', s1 + 1);
+                    if (s2 != std::string::npos && s2 + 1 < tok.size()) ni = std::atoi(tok.c_str() + s2 + 1);
                 }
-                int nv = (int)d.v.size() / 3, nn = (int)d.vn.size() / 3;
                 vi = vi > 0 ? vi - 1 : nv + vi;
                 ni = ni > 0 ? ni - 1 : (ni < 0 ? nn + ni : -1);
                 if (vi < 0 || vi >= nv) throw PcrError(PCR_ERR_SCENE, "Failed to parse OBJ " + path + ": vertex index out of range");
@@ -850,6 +866,7 @@ ObjData load_obj(const std::string& path)
                 d.faces.push_back({idx[0].first, idx[k].first, idx[k + 1].first, idx[0].second, idx[k].second,
                                    idx[k + 1].second});
         }
+        p = eol + 1;
     }
     return d;
 }

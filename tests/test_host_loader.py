@@ -141,3 +141,24 @@ def test_loader_errors_are_reported(capi, tmp_path):
     assert "at least one primitive" in str(e.value)
     with pytest.raises(capi.PcrError):
         capi.HostScene(str(tmp_path / "missing.json"))
+
+
+def test_parallel_host_bvh_build_matches_oracle_on_200k_triangles(capi):
+    """Ranges above 65,536 triangles are binned by several threads and large
+    sibling subtrees are built concurrently; the node arrays and the
+    triangle order must equal the oracle's sequential restatement of the
+    reference builder."""
+    from oracle import oracle as O
+    from pcr_b200 import workloads
+    O.build()
+    path = workloads.mesh_scene(100, 5)
+    hs = capi.HostScene(path, GOLDEN)
+    tl, ids = hs.triangles(), hs.triangle_ids()
+    assert tl.shape[0] == 200_000
+    tris = np.zeros((tl.shape[0], 9), np.float32)
+    tris[ids] = tl[:, :9]
+    boxes, ints, perm, _, _ = O.bvh_build(tris)
+    b = hs.bvh()
+    assert np.array_equal(b[:, :6].view(np.uint32), boxes.view(np.uint32))
+    assert np.array_equal(b[:, 6:].view(np.int32), ints)
+    assert np.array_equal(ids, perm)
