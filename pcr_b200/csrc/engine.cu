@@ -1091,14 +1091,27 @@ void Engine::serve_loop()
             }
         }
     } catch (const std::exception& e) {
+        // waiters learn of it at once instead of running into their timeout
+        const PcrError* pe = dynamic_cast<const PcrError*>(&e);
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            serve_error_ = e.what();
+            serve_status_ = pe ? pe->status : PCR_ERR_CUDA;
+        }
         std::fprintf(stderr, "pcr: serve loop stopped: %s\n", e.what());
         serving_ = false;
+        cv_done_.notify_all();
     }
 }
 
 void Engine::serve_start()
 {
     if (serving_) return;
+    if (serve_thread_.joinable()) serve_thread_.join();  // a loop that stopped on an error
+    {
+        std::lock_guard<std::mutex> l(mu_);
+        serve_error_.clear();
+    }
     stop_ = false;
     serving_ = true;
     serve_thread_ = std::thread([this] { serve_loop(); });
@@ -1131,6 +1144,10 @@ void Engine::wait(int64_t id, int64_t timeout_ms)
     auto deadline = std::chrono::steady_clock::now() + std::chrono::milliseconds(timeout_ms < 0 ? (int64_t)1 << 40 : timeout_ms);
     while (!poll(id)) {
         if (std::chrono::steady_clock::now() > deadline) throw PcrError(PCR_ERR_TIMEOUT, "wait timed out");
+        {
+            std::lock_guard<std::mutex> l(mu_);
+            if (!serve_error_.empty()) throw PcrError(serve_status_, "serve loop stopped: " + serve_error_);
+        }
         if (!serving_) {
             std::lock_guard<std::mutex> g(run_mu_);
             if (!engine_step()) {

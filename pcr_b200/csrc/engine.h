@@ -201,6 +201,8 @@ private:
     bool active_dirty_ = true;
     std::thread serve_thread_;
     std::atomic<bool> serving_{false}, stop_{false};
+    std::string serve_error_;                 // why the serve loop stopped (guarded by mu_)
+    pcr_status serve_status_ = PCR_OK;
     std::mutex run_mu_;   // one driver of the device loop at a time
 
     // stats

@@ -185,3 +185,27 @@ def test_pending_requests_are_admitted_by_priority():
         assert q["f"] < q["a"] < q["c"] < q["e"] < q["b"], q
     finally:
         ctx.close()
+
+
+def test_wait_times_out_and_serving_restarts():
+    """A bounded wait on an unfinished request returns PCR_ERR_TIMEOUT and
+    leaves it running; the serve loop can be stopped and started again and
+    the request then completes unchanged."""
+    from pcr_b200 import capi
+    ctx = capi.Context(device=0, queue_capacity=1 << 17)
+    try:
+        sid = ctx.load_scene_json(scene_path("cornell-glass"), GOLDEN)
+        d = capi.render_desc(384, depth=8, samples=48, shadow=4, seed=44)
+        ref = ctx.render(sid, d)[0]
+        rid = ctx.submit(sid, d)
+        with pytest.raises(capi.PcrError) as e:
+            ctx.wait(rid, 1)
+        assert e.value.status == 6
+        ctx.serve_start()
+        ctx.serve_stop()
+        ctx.serve_start()
+        ctx.wait(rid, 120_000)
+        ctx.serve_stop()
+        assert np.allclose(ctx.fetch(rid)[0], ref, rtol=RTOL, atol=ATOL)
+    finally:
+        ctx.close()
