@@ -313,7 +313,10 @@ __device__ __forceinline__ void prefetch_l2(const void* p)
 #ifndef PCR_TRACE_MIN_BLOCKS
 #define PCR_TRACE_MIN_BLOCKS 4
 #endif
-constexpr int kTraceMaxBlock = 256, kTraceMinBlocks = PCR_TRACE_MIN_BLOCKS;
+#ifndef PCR_SHADOW_MIN_BLOCKS
+#define PCR_SHADOW_MIN_BLOCKS PCR_TRACE_MIN_BLOCKS
+#endif
+constexpr int kTraceMaxBlock = 256, kTraceMinBlocks = PCR_TRACE_MIN_BLOCKS, kShadowMinBlocks = PCR_SHADOW_MIN_BLOCKS;
 
 // Closest hit for every queued path (trace_closest).
 __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(EngineView E, int cur)
@@ -787,7 +790,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
 // 1e-3 (compared in double, as the reference's double literal promotes it);
 // scene_blocked answers it with an early exit.  Lit samples add their XYZ
 // contribution to the pixel's FP64 accumulator.
-__global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_shadow(EngineView E)
+__global__ void __launch_bounds__(kTraceMaxBlock, kShadowMinBlocks) k_shadow(EngineView E)
 {
     Counters* C = E.cnt;
     const int n = min(C->shadow_n, E.shadow_cap);
