@@ -46,7 +46,7 @@ HBM_FALLBACK = 6650.0
 # 8-render step, divided by that step's rays / shadow rays; the summary and
 # command are kept in the profiles directory).  Traffic grows in proportion to
 # the units, so a launch's traffic is this figure times its units.
-NCU_DRAM_PER_UNIT = {"extend": 48.8, "shade": 410.3, "shadow": 67.6}
+NCU_DRAM_PER_UNIT = {"extend": 48.8, "shade": 409.3, "shadow": 67.6}
 
 
 def args_():
