@@ -341,18 +341,6 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(Engi
 
 // ------------------------------------------------------------------ helpers
 
-__device__ __forceinline__ int warp_append(int* counter, bool want)
-{
-    const unsigned mask = __ballot_sync(0xffffffffu, want);
-    if (mask == 0) return -1;
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(mask) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(counter, __popc(mask));
-    base = __shfl_sync(0xffffffffu, base, leader);
-    return want ? base + __popc(mask & ((1u << lane) - 1u)) : -1;
-}
-
 __device__ __forceinline__ void add_xyz(double* acc, float3 c)
 {
     atomicAdd(acc + 0, (double)c.x);
