@@ -181,6 +181,10 @@ void Engine::alloc_buffers()
     d_round_list_ = dalloc<int>(kMaxActive, T);
     d_cnt_ = dalloc<Counters>(1, T);
     d_params_ = dalloc<EngineParams>(1, T);
+    d_cmf_ = dalloc<float4>(kCmfEntries, T);
+    k_cmf_table<<<(kCmfEntries + 255) / 256, 256, 0, stream_>>>(d_cmf_);
+    CK(cudaGetLastError());
+    CK(cudaStreamSynchronize(stream_));
     CK(cudaMemset(d_issued_, 0, 8 * kMaxActive));
     CK(cudaMemset(d_outstanding_, 0, 8 * kMaxActive));
     CK(cudaMemset(d_done_, 0, 4 * kMaxActive));
@@ -289,6 +293,7 @@ EngineView Engine::view() const
     E.round_state = d_round_state_;
     E.round_cnt = d_round_cnt_;
     E.round_list = d_round_list_;
+    E.cmf_table = d_cmf_;
     return E;
 }
 
@@ -1467,6 +1472,7 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     E.round_state = round_state;
     E.round_cnt = round_cnt;
     E.round_list = round_list;
+    E.cmf_table = d_cmf_;
     E.queue_cap = kNoAllocQueue;
     E.n_mats = mat_count_;
 

@@ -151,6 +151,7 @@ private:
     long long* d_give_start_ = nullptr;
     int *d_give_ = nullptr, *d_give_base_ = nullptr, *d_active_ = nullptr, *d_nactive_ = nullptr, *d_done_ = nullptr;
     int *d_round_state_ = nullptr, *d_round_cnt_ = nullptr, *d_round_list_ = nullptr;
+    float4* d_cmf_ = nullptr;  // colour-matching table for raygen
     int* h_active_ = nullptr;     // pinned: [0] = n, then slots
     Counters* d_cnt_ = nullptr;
     struct HostSnap {

@@ -120,13 +120,38 @@ __global__ void __launch_bounds__(kSchedThreads) k_schedule(EngineView E, const 
 // (700-400)/yBarIntegral / N, so the pixel contribution of per-channel
 // radiance c is sum_k c_k w_k = sum_k singleLambdaXYZ(lam_k, c_k) / N
 // (code/Renderer.cpp:254-257, code/Includes/CIE.h:140-159).  Computed once
-// per vertex; RGB mode passes the channels through.
+// per path at raygen; RGB mode passes the channels through.
 struct XyzWeights {
     float3 w[4];
 };
-// Kept out of line: seven double-precision exponentials per wavelength make
-// a large body, and one shared copy keeps k_shade's instruction footprint small.
-__device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale)
+
+// The colour-matching functions tabulated at kCmfStep nm over [400, 700]
+// from the exact device cmf() (seven correctly rounded exponentials per
+// wavelength), read back with linear interpolation.  The interpolation
+// error is below 1e-7 of each function's peak and below 5e-6 relative
+// (the worst case is x-bar near 500 nm, where its lobes cancel), and raygen
+// evaluates four wavelengths per path without 28 double-precision
+// exponentials.
+constexpr float kCmfStep = 0.0125f;
+constexpr int kCmfEntries = 24001;  // (700 - 400) / kCmfStep + 1
+__global__ void k_cmf_table(float4* table)
+{
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kCmfEntries; i += gridDim.x * blockDim.x) {
+        const float3 c = cmf(400.f + (float)i * kCmfStep);
+        table[i] = make_float4(c.x, c.y, c.z, 0.f);
+    }
+}
+__device__ __forceinline__ float3 cmf_lut(const float4* __restrict__ table, float l)
+{
+    const float t = fminf(fmaxf((l - 400.f) * (1.f / kCmfStep), 0.f), (float)(kCmfEntries - 1));
+    const int i = min((int)t, kCmfEntries - 2);
+    const float f = t - (float)i;
+    const float4 a = table[i], b = table[i + 1];
+    return make_float3(a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f, a.z + (b.z - a.z) * f);
+}
+
+__device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale,
+                                               const float4* cmf_table)
 {
     XyzWeights W;
     if (!spectral) {
@@ -138,7 +163,7 @@ __device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, 
     }
     for (int k = 0; k < 4; k++) {
         if (k < nch) {
-            float3 c = cmf(lam[k]);
+            float3 c = cmf_lut(cmf_table, lam[k]);
             const float s = xyz_scale * wN;
             W.w[k] = make_float3(c.x * s, c.y * s, c.z * s);
         } else {
@@ -280,7 +305,7 @@ __global__ void k_regen(EngineView E, int cur, float xyz_scale)
                 if (l > 700.f) l -= span;
                 lam[k] = k < nch ? l : lam[0];
             }
-            XyzWeights W = xyz_weights(true, lam, nch, 1.f / (float)nch, xyz_scale);
+            XyzWeights W = xyz_weights(true, lam, nch, 1.f / (float)nch, xyz_scale, E.cmf_table);
             const DScene& S = E.scenes[R.scene];
             if (S.emit_mat >= 0) {
                 // emission of the scene's only emissive material, folded in

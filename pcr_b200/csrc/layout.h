@@ -191,6 +191,7 @@ struct EngineView {
     int* round_state;                // per slot: 1 while an adaptive round's per-pixel step is pending
     int* round_cnt;                  // per slot: pixels kept for the next adaptive round
     int* round_list;                 // slots of Counters::n_rounds
+    const float4* cmf_table;         // CIE colour-matching functions at fine spacing (raygen)
 };
 
 }  // namespace pcr
