@@ -46,3 +46,27 @@ def test_cli_rejects_unknown_scene():
     out = subprocess.run([CLI, "--scenes-dir", os.path.join(GOLDEN, "scenes"), "--scene", "nope"],
                          capture_output=True, text=True, timeout=60)
     assert out.returncode == 1 and "Unknown scene" in out.stderr
+
+
+def test_cli_denoise_adaptive_aces_match_library(tmp_path):
+    """--denoise, --aa-samples with --adaptive and --aces go through the same
+    device paths as the library call with those knobs."""
+    from PIL import Image
+
+    from pcr_b200 import capi
+    args = [CLI, "--scenes-dir", os.path.join(GOLDEN, "scenes"), "--scene", "cornell-spheres", "-w", "40",
+            "--height", "32", "-d", "3", "-s", "4", "-S", "2", "--spectral", "--seed", "5", "--denoise", "--aa",
+            "--aa-samples", "6", "--adaptive", "--aces", "-o", str(tmp_path)]
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    files = os.listdir(tmp_path)
+    assert len(files) == 1 and "-aces-" in files[0]
+    img = Image.open(tmp_path / files[0])
+    assert img.text["Adaptive"] == "1" and img.text["Denoise"] == "1"
+    rgb = np.asarray(img.convert("RGB"))
+    ctx = capi.Context()
+    sid = ctx.load_scene_json(scene_path("cornell-spheres"), GOLDEN)
+    _, lib_rgb, _ = ctx.render(sid, capi.render_desc(40, 32, depth=3, samples=4, shadow=2, spectral=True, seed=5,
+                                                     denoise=True, aa=6, adaptive=True, aces=True))
+    ctx.close()
+    assert np.array_equal(rgb, lib_rgb)
