@@ -279,6 +279,15 @@ pcr_status pcr_router_load(pcr_router *r, int64_t *outstanding_paths, int64_t *r
  * non-emissive and closer than light_dist2 - 1e-3 (compared in double). */
 pcr_status pcr_trace_shadow(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, const float *light_dist2,
                             int64_t n, int32_t *blocked);
+/* Bvh::build (code/Bvh/Bvh.cpp:122-325) on the context's device: the binary
+ * SAH tree over tris[0..n) in the reference's depth-first layout, equal bit
+ * for bit to the host builder's, and order_out[i] = index in `tris` of the
+ * triangle at leaf position i (the reference permutes its triangle vector in
+ * place; tris here is left as it is).  nodes_out holds max_nodes entries
+ * (2n - 1 always suffices); *n_nodes receives the count.  Synchronous.
+ * pcr_scene_upload runs this builder when the descriptor has no BVH. */
+pcr_status pcr_bvh_build(pcr_ctx *ctx, const pcr_triangle *tris, int32_t n, pcr_bvh_node *nodes_out,
+                         int32_t max_nodes, int32_t *n_nodes, int32_t *order_out);
 /* Device evaluations of the FP32 stage functions on a wavelength / colour grid:
  * what 0 sigmoid fit at lambda (fit=4 floats) | 1 tabulated spectrum (61) |
  * 2 CIE xbar/ybar/zbar (3 out) | 3 singleLambdaXYZ(lambda, in[i]) (3 out) |

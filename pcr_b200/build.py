@@ -22,8 +22,8 @@ LIB = os.path.join(LIBDIR, "libpcr_b200.so")
 CLI = os.path.join(LIBDIR, "pcr-render")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["engine.cu", "scene.cpp", "capi.cpp"]
-HEADERS = ["layout.h", "device.cuh", "kernels.cuh", "engine.h", "scene.h"]
+SOURCES = ["engine.cu", "bvh_build.cu", "scene.cpp", "capi.cpp"]
+HEADERS = ["layout.h", "device.cuh", "kernels.cuh", "engine.h", "scene.h", "bvh_build.h"]
 
 
 def _newer(target: str, deps) -> bool:

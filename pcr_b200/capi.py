@@ -26,7 +26,7 @@ EXPORTS = [
     "pcr_fit_sigmoid", "pcr_lut_build", "pcr_scene_release", "pcr_scene_bytes", "pcr_render", "pcr_render_noalloc",
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
     "pcr_fetch", "pcr_cancel", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
-    "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_eval_stage",
+    "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_bvh_build", "pcr_eval_stage",
     "pcr_tonemap", "pcr_router_create", "pcr_router_destroy", "pcr_router_scene_load_json", "pcr_router_serve_start",
     "pcr_router_serve_stop", "pcr_router_submit", "pcr_router_wait", "pcr_router_fetch", "pcr_router_load",
 ]
@@ -157,6 +157,7 @@ def load_library():
         "pcr_trace_closest": [P, C.c_int32, fp, C.c_int64, ip, ip, fp],
         "pcr_trace_bvh": [P, C.c_int32, fp, C.c_int64, ip, fp, ip],
         "pcr_trace_shadow": [P, C.c_int32, fp, fp, C.c_int64, ip],
+        "pcr_bvh_build": [P, fp, C.c_int32, fp, C.c_int32, ip, ip],
         "pcr_tonemap": [P, fp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, C.POINTER(C.c_uint8)],
         "pcr_router_create": [C.POINTER(P), C.POINTER(P), C.c_int32],
         "pcr_router_destroy": [P],
@@ -436,6 +437,20 @@ class Context:
         out = np.zeros(n, np.int32)
         _check(self.L.pcr_trace_shadow(self.h, sid, _fp(r), _fp(d2), n, _ip(out)))
         return out
+
+    def build_bvh(self, verts: np.ndarray):
+        """Device SAH build over n triangles given as (n, 9) vertices
+        (v0 v1 v2): returns (nodes as (m, 9) float32 rows with the last
+        three words int32, order) like HostScene.bvh() / triangle_ids()."""
+        v = np.ascontiguousarray(verts, np.float32).reshape(-1, 9)
+        n = v.shape[0]
+        tris = np.zeros((n, 23), np.float32)
+        tris[:, :9] = v
+        nodes = np.zeros((max(2 * n - 1, 1), 9), np.float32)
+        order = np.zeros(n, np.int32)
+        m = C.c_int32(0)
+        _check(self.L.pcr_bvh_build(self.h, _fp(tris), n, _fp(nodes), nodes.shape[0], C.byref(m), _ip(order)))
+        return nodes[:m.value].copy(), order
 
     def tonemap(self, hdr: np.ndarray, aces=False, denoise=False) -> np.ndarray:
         """8-bit image of a linear sRGB image (H, W, 3), on the device."""

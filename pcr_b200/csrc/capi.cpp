@@ -65,7 +65,8 @@ std::string parent_dir(const std::string& p)
     return k == std::string::npos ? std::string(".") : (k == 0 ? std::string("/") : p.substr(0, k));
 }
 
-pcr::HostScene host_scene_from_json(const char* path, const char* data_root, const char* lut_path)
+pcr::HostScene host_scene_from_json(const char* path, const char* data_root, const char* lut_path,
+                                    bool with_bvh = true)
 {
     // default data root: the directory that holds the scene directory
     // (the reference ships <root>/Scenes/*.json beside <root>/spd/)
@@ -76,7 +77,25 @@ pcr::HostScene host_scene_from_json(const char* path, const char* data_root, con
         if (!pcr::load_plut(lut_path, lut, &err))
             throw pcr::PcrError(PCR_ERR_SCENE, std::string("loadLUT(") + lut_path + "): " + err);
     }
-    return pcr::load_scene_json(path, root, lut_path ? &lut : nullptr);
+    return pcr::load_scene_json(path, root, lut_path ? &lut : nullptr, with_bvh);
+}
+
+// The BVH of a scene loaded without one, built on `e`'s device; the
+// triangles and their ids are put into leaf order as the host builder does.
+void device_bvh(pcr::Engine& e, pcr::HostScene& s)
+{
+    const int n = (int)s.triangles.size();
+    if (n == 0) return;
+    std::vector<int32_t> order;
+    e.build_bvh(s.triangles.data(), n, s.bvh, order);
+    std::vector<pcr_triangle> t(n);
+    std::vector<int32_t> ids(n);
+    for (int i = 0; i < n; i++) {
+        t[i] = s.triangles[order[i]];
+        ids[i] = s.triangle_ids[order[i]];
+    }
+    s.triangles.swap(t);
+    s.triangle_ids.swap(ids);
 }
 }  // namespace
 
@@ -128,7 +147,8 @@ pcr_status pcr_scene_load_json(pcr_ctx* ctx, const char* path, const char* data_
 {
     return guard([&] {
         if (!path || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
-        pcr::HostScene s = host_scene_from_json(path, data_root, lut_path);
+        pcr::HostScene s = host_scene_from_json(path, data_root, lut_path, false);
+        device_bvh(E(ctx), s);
         pcr_scene_desc d = s.desc();
         *out = E(ctx).upload_scene(d);
     });
@@ -334,7 +354,8 @@ pcr_status pcr_router_scene_load_json(pcr_router* r, const char* path, const cha
     return guard([&] {
         pcr_router& R = RT(r);
         if (!path || !out) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
-        pcr::HostScene hs = host_scene_from_json(path, data_root, lut_path);
+        pcr::HostScene hs = host_scene_from_json(path, data_root, lut_path, false);
+        device_bvh(*R.eng[0], hs);   // built once, uploaded to every context
         const pcr_scene_desc d = hs.desc();
         std::vector<int> ids;
         for (pcr::Engine* e : R.eng) ids.push_back(e->upload_scene(d));
@@ -427,6 +448,22 @@ pcr_status pcr_trace_shadow(pcr_ctx* ctx, pcr_scene_id scene, const float* rays,
     return guard([&] {
         if ((!rays || !light_dist2 || !blocked) && n > 0) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
         E(ctx).trace_shadow(scene, rays, light_dist2, n, blocked);
+    });
+}
+
+pcr_status pcr_bvh_build(pcr_ctx* ctx, const pcr_triangle* tris, int32_t n, pcr_bvh_node* nodes_out,
+                         int32_t max_nodes, int32_t* n_nodes, int32_t* order_out)
+{
+    return guard([&] {
+        if (n < 0 || max_nodes < 0) throw pcr::PcrError(PCR_ERR_INVALID, "negative count");
+        if (!n_nodes || (n > 0 && (!tris || !order_out || !nodes_out))) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        std::vector<pcr_bvh_node> nodes;
+        std::vector<int32_t> order;
+        E(ctx).build_bvh(tris, n, nodes, order);
+        if ((int64_t)nodes.size() > max_nodes) throw pcr::PcrError(PCR_ERR_INVALID, "nodes_out too small");
+        std::copy(nodes.begin(), nodes.end(), nodes_out);
+        std::copy(order.begin(), order.end(), order_out);
+        *n_nodes = (int32_t)nodes.size();
     });
 }
 

@@ -6,6 +6,7 @@
 #include <cstring>
 #include <numeric>
 
+#include "bvh_build.h"
 #include "kernels.cuh"
 #include "scene.h"
 
@@ -392,7 +393,8 @@ int Engine::upload_scene(const pcr_scene_desc& d)
     std::memcpy(e.cam, d.cam_pos, sizeof(e.cam));
     e.fov = d.fov;
 
-    // triangles + BVH (built here with the reference's builder when absent)
+    // triangles + BVH (built here on the device, equal to the reference's
+    // builder, when the descriptor has none)
     std::vector<pcr_triangle> tris(d.triangles, d.triangles + d.n_triangles);
     std::vector<int32_t> ids(d.n_triangles);
     for (int i = 0; i < d.n_triangles; i++) ids[i] = d.triangle_ids ? d.triangle_ids[i] : i;
@@ -401,7 +403,7 @@ int Engine::upload_scene(const pcr_scene_desc& d)
         if (d.n_bvh_nodes > 0 && d.bvh_nodes)
             bvh.assign(d.bvh_nodes, d.bvh_nodes + d.n_bvh_nodes);
         else
-            bvh = build_bvh(tris, &ids);
+            bvh = device_build_bvh(device_, stream_, pool_, tris, &ids);
     }
     for (const auto& n : bvh)
         if (n.count == 0 && (n.left_or_first < 0 || n.left_or_first >= (int)bvh.size() || n.right_child < 0 ||
@@ -1581,6 +1583,19 @@ void Engine::record_other(cudaEvent_t a, cudaEvent_t z)
     CK(cudaEventElapsedTime(&ms, a, z));
     stage_ms_[7] += ms;
     stage_launches_[7]++;
+}
+
+void Engine::build_bvh(const pcr_triangle* tris, int n, std::vector<pcr_bvh_node>& nodes, std::vector<int32_t>& order)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    std::vector<float> v((size_t)n * 9);
+    for (int i = 0; i < n; i++)
+        for (int a = 0; a < 3; a++) {
+            v[(size_t)i * 9 + a] = tris[i].v0[a];
+            v[(size_t)i * 9 + 3 + a] = tris[i].v1[a];
+            v[(size_t)i * 9 + 6 + a] = tris[i].v2[a];
+        }
+    device_build_bvh_raw(device_, stream_, pool_, v.data(), n, nodes, order);
 }
 
 void Engine::trace_shadow(int scene, const float* rays, const float* dist2, int64_t n, int32_t* blocked)

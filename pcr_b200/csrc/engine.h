@@ -91,6 +91,7 @@ public:
                int32_t* counts);
     void record_other(cudaEvent_t a, cudaEvent_t z);
     void trace_shadow(int scene, const float* rays, const float* dist2, int64_t n, int32_t* blocked);
+    void build_bvh(const pcr_triangle* tris, int n, std::vector<pcr_bvh_node>& nodes, std::vector<int32_t>& order);
     void tonemap(const float* hdr, int width, int height, int aces_tm, int denoise, uint8_t* rgb8);
     void eval_stage(int what, const float* params, const float* in, int64_t n, float* out);
 

@@ -900,7 +900,8 @@ std::string req_str(const JVal& p, const char* key, const std::string& where)
 }  // namespace
 
 // ============================================================ scene assembly
-HostScene load_scene_json(const std::string& path, const std::string& data_root, const std::vector<float>* lut)
+HostScene load_scene_json(const std::string& path, const std::string& data_root, const std::vector<float>* lut,
+                          bool with_bvh)
 {
     const std::string text = read_file(path);
     JParser P(text, path);
@@ -1138,7 +1139,7 @@ HostScene load_scene_json(const std::string& path, const std::string& data_root,
     S.planes.insert(S.planes.end(), walls.begin(), walls.end());
     S.triangle_ids.resize(S.triangles.size());
     for (size_t i = 0; i < S.triangles.size(); i++) S.triangle_ids[i] = (int32_t)i;
-    S.bvh = build_bvh(S.triangles, &S.triangle_ids);
+    if (with_bvh) S.bvh = build_bvh(S.triangles, &S.triangle_ids);
     for (auto& m : S.materials) populate_material(m, lut);
     return S;
 }

@@ -40,7 +40,10 @@ struct HostScene {
 
 // Scene JSON schema 1.x with // and /* */ comments (code/Scenes/SceneLoader.cpp:475-516).
 // data_root holds spd/<name>.spd; lut (3*16^3*3 floats) selects the LUT fit.
-HostScene load_scene_json(const std::string& path, const std::string& data_root, const std::vector<float>* lut);
+// with_bvh = false leaves the triangles in file order and the BVH empty (for
+// a build on the device).
+HostScene load_scene_json(const std::string& path, const std::string& data_root, const std::vector<float>* lut,
+                          bool with_bvh = true);
 
 // Bvh::build (code/Bvh/Bvh.cpp:95-391): 16-bin SAH on centroids, leaf <= 4,
 // depth-first layout; permutes tris (and ids) into leaf order.
