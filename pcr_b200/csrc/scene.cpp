@@ -6,6 +6,7 @@
 
 #include <algorithm>
 #include <array>
+#include <charconv>
 #include <cfloat>
 #include <functional>
 #include <cmath>
@@ -18,6 +19,10 @@
 #include <stdexcept>
 #include <future>
 #include <thread>
+
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
 
 #include "engine.h"
 
@@ -813,21 +818,53 @@ struct ObjData {
     std::vector<std::array<int, 6>> faces;  // v0 v1 v2 n0 n1 n2 (n = -1 when absent)
 };
 
-// Wavefront OBJ subset the reference's loader reads (v, vn, f with v,
-// v/t, v//n, v/t/n tokens, fans of polygons).  The whole file is read at
-// once and scanned in place; numbers go through strtod / strtol, as before.
-ObjData load_obj(const std::string& path)
+// strtod on the OBJ number fields: blanks (newline included, as strtod's
+// isspace) are skipped, then std::from_chars reads the number (correctly
+// rounded, as strtod); the rare forms from_chars does not take (hex,
+// out-of-range values) go to strtod itself.  No number: 0, pointer unmoved.
+inline double scan_double(const char*& q, const char* end)
 {
-    std::ifstream in(path, std::ios::binary | std::ios::ate);
-    if (!in) throw PcrError(PCR_ERR_SCENE, "Mesh file not found: " + path);
-    const std::streamsize size = in.tellg();
-    in.seekg(0);
-    std::string buf((size_t)std::max<std::streamsize>(size, 0), '\0');
-    if (size > 0 && !in.read(&buf[0], size)) throw PcrError(PCR_ERR_SCENE, "Failed to read OBJ " + path);
-    buf.push_back('\n');
-    ObjData d;
-    const char* p = buf.c_str();
-    const char* const end = p + buf.size();
+    const char* s = q;
+    while (s < end && (*s == ' ' || *s == '\t' || *s == '\r' || *s == '\n' || *s == '\v' || *s == '\f')) s++;
+    const char* num = s;
+    if (num < end && *num == '+') {
+        num++;
+        if (num < end && (*num == '+' || *num == '-')) return 0.0;
+    }
+    const bool hex = end - num >= 2 && num[0] == '0' && (num[1] == 'x' || num[1] == 'X');
+    double v = 0.0;
+    const auto r = hex ? std::from_chars_result{num, std::errc::invalid_argument} : std::from_chars(num, end, v);
+    if (r.ec == std::errc()) {
+        q = r.ptr;
+        return v;
+    }
+    if (r.ec == std::errc::invalid_argument && !hex) return 0.0;
+    char* e;
+    v = std::strtod(q, &e);   // the buffer is NUL-terminated
+    q = e;
+    return v;
+}
+
+// atoi over one face token's characters
+inline int scan_int(const char* s, const char* end)
+{
+    bool neg = false;
+    if (s < end && (*s == '+' || *s == '-')) neg = *s++ == '-';
+    long long v = 0;
+    while (s < end && *s >= '0' && *s <= '9') v = v * 10 + (*s++ - '0');
+    return (int)(neg ? -v : v);
+}
+
+struct ObjChunk {
+    std::vector<std::array<int, 6>> faces;
+    std::string error;   // first error in this chunk
+};
+
+// One contiguous range of lines; nv / nn = vertices / normals defined
+// before it.  Vertices and normals go straight to their final positions.
+void parse_obj_lines(const char* p, const char* end, int nv, int nn, float* v, float* vn, ObjChunk& out,
+                     const std::string& path)
+{
     std::vector<std::pair<int, int>> idx;
     while (p < end) {
         const char* eol = static_cast<const char*>(std::memchr(p, '\n', (size_t)(end - p)));
@@ -835,39 +872,127 @@ ObjData load_obj(const std::string& path)
         const size_t len = (size_t)(eol - p);
         if (len >= 2 && p[0] == 'v' && p[1] == ' ') {
             const char* q = p + 2;
-            char* e;
-            for (int k = 0; k < 3; k++) { d.v.push_back((float)std::strtod(q, &e)); q = e; }
+            for (int k = 0; k < 3; k++) v[(size_t)nv * 3 + k] = (float)scan_double(q, end);
+            nv++;
         } else if (len >= 3 && p[0] == 'v' && p[1] == 'n' && p[2] == ' ') {
             const char* q = p + 3;
-            char* e;
-            for (int k = 0; k < 3; k++) { d.vn.push_back((float)std::strtod(q, &e)); q = e; }
+            for (int k = 0; k < 3; k++) vn[(size_t)nn * 3 + k] = (float)scan_double(q, end);
+            nn++;
         } else if (len >= 2 && p[0] == 'f' && p[1] == ' ') {
             idx.clear();
             const char* q = p + 2;
-            const int nv = (int)d.v.size() / 3, nn = (int)d.vn.size() / 3;
             while (q < eol) {
                 while (q < eol && (*q == ' ' || *q == '\t' || *q == '\r')) q++;
                 if (q >= eol) break;
                 const char* t0 = q;   // one token: v, v/t, v//n or v/t/n
                 while (q < eol && *q != ' ' && *q != '\t' && *q != '\r') q++;
-                const std::string tok(t0, (size_t)(q - t0));
-                int vi = std::atoi(tok.c_str()), ni = 0;
-                const size_t s1 = tok.find('/');
-                if (s1 != std::string::npos) {
-                    const size_t s2 = tok.find('/', s1 + 1);
-                    if (s2 != std::string::npos && s2 + 1 < tok.size()) ni = std::atoi(tok.c_str() + s2 + 1);
+                int vi = scan_int(t0, q), ni = 0;
+                const char* s1 = static_cast<const char*>(std::memchr(t0, '/', (size_t)(q - t0)));
+                if (s1) {
+                    const char* s2 = static_cast<const char*>(std::memchr(s1 + 1, '/', (size_t)(q - s1 - 1)));
+                    if (s2 && s2 + 1 < q) ni = scan_int(s2 + 1, q);
                 }
                 vi = vi > 0 ? vi - 1 : nv + vi;
                 ni = ni > 0 ? ni - 1 : (ni < 0 ? nn + ni : -1);
-                if (vi < 0 || vi >= nv) throw PcrError(PCR_ERR_SCENE, "Failed to parse OBJ " + path + ": vertex index out of range");
+                if (vi < 0 || vi >= nv) {
+                    out.error = "Failed to parse OBJ " + path + ": vertex index out of range";
+                    return;
+                }
                 idx.emplace_back(vi, ni);
             }
             for (size_t k = 1; k + 1 < idx.size(); k++)
-                d.faces.push_back({idx[0].first, idx[k].first, idx[k + 1].first, idx[0].second, idx[k].second,
-                                   idx[k + 1].second});
+                out.faces.push_back({idx[0].first, idx[k].first, idx[k + 1].first, idx[0].second, idx[k].second,
+                                     idx[k + 1].second});
         }
         p = eol + 1;
     }
+}
+
+// Wavefront OBJ subset the reference's loader reads (v, vn, f with v,
+// v/t, v//n, v/t/n tokens, fans of polygons).  The file is read by several
+// threads at once and cut into ranges of whole lines; a first parallel pass counts the v / vn
+// lines of each range, so the second (also parallel) pass knows how many
+// vertices precede every line (relative indices, range checks) and where
+// its vertices go.  Faces are concatenated in file order and the first
+// error in file order is reported, as a sequential reader would.
+ObjData load_obj(const std::string& path)
+{
+    const int fd = ::open(path.c_str(), O_RDONLY);
+    if (fd < 0) throw PcrError(PCR_ERR_SCENE, "Mesh file not found: " + path);
+    struct stat sb;
+    if (::fstat(fd, &sb) != 0) {
+        ::close(fd);
+        throw PcrError(PCR_ERR_SCENE, "Failed to read OBJ " + path);
+    }
+    const size_t fsize = (size_t)std::max<off_t>(sb.st_size, 0);
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int parts = fsize < (1u << 20) ? 1 : std::min(64, 2 * hw);
+    auto run = [&](int n, auto&& fn) {
+        if (n == 1) { fn(0); return; }
+        std::vector<std::thread> th;
+        const int nt = std::min(n, hw);
+        for (int t = 0; t < nt; t++)
+            th.emplace_back([&, t] { for (int k = t; k < n; k += nt) fn(k); });
+        for (auto& x : th) x.join();
+    };
+    // the file in `parts` ranges read concurrently, then a newline and a NUL
+    std::unique_ptr<char[]> buf(new char[fsize + 2]);
+    std::vector<int> read_ok(parts, 1);
+    run(parts, [&](int k) {
+        size_t o = fsize * (size_t)k / (size_t)parts;
+        const size_t e = fsize * (size_t)(k + 1) / (size_t)parts;
+        while (o < e) {
+            const ssize_t r = ::pread(fd, buf.get() + o, e - o, (off_t)o);
+            if (r <= 0) { read_ok[k] = 0; return; }
+            o += (size_t)r;
+        }
+    });
+    ::close(fd);
+    for (int ok : read_ok)
+        if (!ok) throw PcrError(PCR_ERR_SCENE, "Failed to read OBJ " + path);
+    buf[fsize] = '\n';
+    buf[fsize + 1] = '\0';
+    const char* const b0 = buf.get();
+    const char* const end = b0 + fsize + 1;
+    const size_t bsize = fsize + 1;
+    // range starts on line boundaries
+    std::vector<const char*> cut(parts + 1, end);
+    cut[0] = b0;
+    for (int k = 1; k < parts; k++) {
+        const char* t = b0 + bsize * (size_t)k / (size_t)parts;
+        if (t < cut[k - 1]) t = cut[k - 1];
+        const char* nl = static_cast<const char*>(std::memchr(t, '\n', (size_t)(end - t)));
+        cut[k] = nl ? nl + 1 : end;
+    }
+    std::vector<int> cv(parts, 0), cn(parts, 0);
+    auto count = [&](int k) {
+        for (const char* p = cut[k]; p < cut[k + 1];) {
+            const char* eol = static_cast<const char*>(std::memchr(p, '\n', (size_t)(cut[k + 1] - p)));
+            if (!eol) eol = cut[k + 1];
+            const size_t len = (size_t)(eol - p);
+            if (len >= 2 && p[0] == 'v' && p[1] == ' ') cv[k]++;
+            else if (len >= 3 && p[0] == 'v' && p[1] == 'n' && p[2] == ' ') cn[k]++;
+            p = eol + 1;
+        }
+    };
+    run(parts, count);
+    std::vector<int> v0(parts + 1, 0), n0(parts + 1, 0);
+    for (int k = 0; k < parts; k++) {
+        v0[k + 1] = v0[k] + cv[k];
+        n0[k + 1] = n0[k] + cn[k];
+    }
+    ObjData d;
+    d.v.resize((size_t)v0[parts] * 3);
+    d.vn.resize((size_t)n0[parts] * 3);
+    std::vector<ObjChunk> ch(parts);
+    run(parts, [&](int k) { parse_obj_lines(cut[k], cut[k + 1], v0[k], n0[k], d.v.data(), d.vn.data(), ch[k], path); });
+    size_t nf = 0;
+    for (const auto& c : ch) {
+        if (!c.error.empty()) throw PcrError(PCR_ERR_SCENE, c.error);
+        nf += c.faces.size();
+    }
+    d.faces.reserve(nf);
+    for (const auto& c : ch) d.faces.insert(d.faces.end(), c.faces.begin(), c.faces.end());
     return d;
 }
 
@@ -1079,28 +1204,46 @@ HostScene load_scene_json(const std::string& path, const std::string& data_root,
                 }
             }
             ObjData od = load_obj(scene_dir + "/" + file);
-            const int nv = (int)od.v.size() / 3;
+            const int nv = (int)od.v.size() / 3, nn = (int)od.vn.size() / 3, nf = (int)od.faces.size();
+            for (const auto& f : od.faces)
+                for (int k = 3; k < 6; k++)
+                    if (f[k] >= nn) throw PcrError(PCR_ERR_SCENE, "Failed to parse OBJ " + file + ": normal index out of range");
+            // per-vertex, per-normal and per-face work is independent: split
+            // over host threads (same arithmetic per element)
+            const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+            auto par = [&](int n, auto&& fn) {
+                const int parts = n < (1 << 16) ? 1 : std::min(16, hw);
+                if (parts == 1) fn(0, 0, n);
+                else parallel_chunks(0, n, parts, fn);
+            };
             std::vector<float> tv(od.v.size()), tn(od.vn.size());
-            for (int k = 0; k < nv; k++) {
-                float v[3] = {od.v[k * 3] * sc[0], od.v[k * 3 + 1] * sc[1], od.v[k * 3 + 2] * sc[2]};
-                rotate_xyz(v, rot);
-                tv[k * 3] = v[0] + pos[0]; tv[k * 3 + 1] = v[1] + pos[1]; tv[k * 3 + 2] = v[2] + pos[2];
-            }
-            for (size_t k = 0; k < od.vn.size() / 3; k++) {
-                float v[3] = {od.vn[k * 3], od.vn[k * 3 + 1], od.vn[k * 3 + 2]};
-                rotate_xyz(v, rot);
-                float m = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
-                tn[k * 3] = v[0] / m; tn[k * 3 + 1] = v[1] / m; tn[k * 3 + 2] = v[2] / m;
-            }
+            par(nv, [&](int, int lo, int hi) {
+                for (int k = lo; k < hi; k++) {
+                    float v[3] = {od.v[k * 3] * sc[0], od.v[k * 3 + 1] * sc[1], od.v[k * 3 + 2] * sc[2]};
+                    rotate_xyz(v, rot);
+                    tv[k * 3] = v[0] + pos[0]; tv[k * 3 + 1] = v[1] + pos[1]; tv[k * 3 + 2] = v[2] + pos[2];
+                }
+            });
+            par(nn, [&](int, int lo, int hi) {
+                for (int k = lo; k < hi; k++) {
+                    float v[3] = {od.vn[k * 3], od.vn[k * 3 + 1], od.vn[k * 3 + 2]};
+                    rotate_xyz(v, rot);
+                    float m = std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+                    tn[k * 3] = v[0] / m; tn[k * 3 + 1] = v[1] / m; tn[k * 3 + 2] = v[2] / m;
+                }
+            });
             const size_t begin = S.triangles.size();
-            for (const auto& f : od.faces) {
-                const bool have_n = f[3] >= 0 && f[4] >= 0 && f[5] >= 0 && smooth;
-                if (have_n)
-                    S.triangles.push_back(make_triangle(&tv[f[0] * 3], &tv[f[1] * 3], &tv[f[2] * 3], &tn[f[3] * 3],
-                                                        &tn[f[4] * 3], &tn[f[5] * 3], mi));
-                else
-                    S.triangles.push_back(make_triangle(&tv[f[0] * 3], &tv[f[1] * 3], &tv[f[2] * 3], nullptr, nullptr, nullptr, mi));
-            }
+            S.triangles.resize(begin + (size_t)nf);
+            par(nf, [&](int, int lo, int hi) {
+                for (int k = lo; k < hi; k++) {
+                    const auto& f = od.faces[k];
+                    const bool have_n = f[3] >= 0 && f[4] >= 0 && f[5] >= 0 && smooth;
+                    S.triangles[begin + k] =
+                        have_n ? make_triangle(&tv[f[0] * 3], &tv[f[1] * 3], &tv[f[2] * 3], &tn[f[3] * 3], &tn[f[4] * 3],
+                                               &tn[f[5] * 3], mi)
+                               : make_triangle(&tv[f[0] * 3], &tv[f[1] * 3], &tv[f[2] * 3], nullptr, nullptr, nullptr, mi);
+                }
+            });
             if (is_light) {
                 light_kind.push_back(1);
                 light_ref.push_back((int)tri_lights.size());

@@ -162,3 +162,75 @@ def test_parallel_host_bvh_build_matches_oracle_on_200k_triangles(capi):
     assert np.array_equal(b[:, :6].view(np.uint32), boxes.view(np.uint32))
     assert np.array_equal(b[:, 6:].view(np.int32), ints)
     assert np.array_equal(ids, perm)
+
+
+def test_parallel_obj_reader_matches_oracle_reader(capi, tmp_path):
+    """An OBJ over 1 MB is read by several threads in ranges of lines:
+    relative (negative) indices, polygon fans, v//n and v/t/n tokens, signed
+    and exponent number forms, and vertices interleaved with faces across
+    range boundaries must give the triangles a sequential reader gives."""
+    from oracle import oracle as O
+    O.build()
+    rng = np.random.default_rng(21)
+    lines = []
+    nv = nn = 0
+    while len(lines) < 60000:
+        k = int(rng.integers(3, 6))
+        for _ in range(k):
+            x = rng.uniform(-1, 1, 3)
+            fmt = rng.integers(0, 3)
+            if fmt == 0:
+                lines.append("v %.9g %.9g %.9g" % tuple(x))
+            elif fmt == 1:
+                lines.append("v %+.6e %+.6e %+.6e" % tuple(x))
+            else:
+                lines.append("v  %.4f\t%.4f %.4f " % tuple(x))
+            n = rng.normal(size=3)
+            lines.append("vn %.7f %.7f %.7f" % tuple(n / np.linalg.norm(n)))
+            nv += 1
+            nn += 1
+        form = rng.integers(0, 4)
+        toks = []
+        for j in range(k):
+            vi = nv - k + j + 1
+            ni = nn - k + j + 1
+            if form == 0:
+                toks.append(str(vi))
+            elif form == 1:
+                toks.append(f"{vi - nv - 1}//{ni - nn - 1}")   # relative
+            elif form == 2:
+                toks.append(f"{vi}/1/{ni}")
+            else:
+                toks.append(f"{vi}//{ni}")
+        lines.append("f " + " ".join(toks))
+        if rng.random() < 0.01:
+            lines.append("# comment line")
+    obj = tmp_path / "m.obj"
+    obj.write_text("vt 0 0\n" + "\n".join(lines) + "\n")
+    assert obj.stat().st_size > (1 << 20)
+    scene = tmp_path / "s.json"
+    scene.write_text('{"schema": "1.0", "name": "m", "version": "1", "materials": {"w": {"albedo": [0.5,0.5,0.5]},'
+                     ' "l": {"emissive": [1,1,1]}}, "primitives": [{"type": "mesh", "file": "m.obj", "material": "w",'
+                     ' "position": [0.1, -0.2, -3], "rotation": [10, 20, 30], "scale": 0.7},'
+                     ' {"type": "plane", "light": true, "origin": [0,2,0], "u": [1,0,0], "v": [0,0,1], "material": "l"}]}')
+    hs = capi.HostScene(str(scene), str(tmp_path))
+    osc = O.load_scene(str(scene), str(tmp_path))
+    mine = hs.triangles()   # both in BVH-leaf order
+    ref = np.array([np.concatenate([np.asarray(t.v0), t.v1, t.v2, t.n0, t.n1, t.n2, t.flatN]).astype(np.float32)
+                    for t in osc.triangles])
+    assert mine.shape[0] == ref.shape[0] > 10000
+    assert np.array_equal(mine[:, :21].view(np.uint32), ref.view(np.uint32))
+    assert np.array_equal(mine[:, 21].view(np.int32), np.array([t.smooth for t in osc.triangles], np.int32))
+    hs.close()
+
+
+def test_obj_normal_index_out_of_range_is_an_error(capi, tmp_path):
+    obj = tmp_path / "m.obj"
+    obj.write_text("v 0 0 0\nv 1 0 0\nv 0 1 0\nvn 0 0 1\nf 1//1 2//1 3//2\n")
+    scene = tmp_path / "s.json"
+    scene.write_text('{"schema": "1.0", "name": "m", "version": "1", "materials": {"w": {"albedo": [0.5,0.5,0.5]},'
+                     ' "l": {"emissive": [1,1,1]}}, "primitives": [{"type": "mesh", "file": "m.obj", "material": "w"},'
+                     ' {"type": "plane", "light": true, "origin": [0,2,0], "u": [1,0,0], "v": [0,0,1], "material": "l"}]}')
+    with pytest.raises(capi.PcrError) as e:
+        capi.HostScene(str(scene), str(tmp_path))
+    assert "normal index out of range" in str(e.value)
