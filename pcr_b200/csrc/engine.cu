@@ -395,15 +395,23 @@ int Engine::upload_scene(const pcr_scene_desc& d)
 
     // triangles + BVH (built here on the device, equal to the reference's
     // builder, when the descriptor has none)
-    std::vector<pcr_triangle> tris(d.triangles, d.triangles + d.n_triangles);
-    std::vector<int32_t> ids(d.n_triangles);
-    for (int i = 0; i < d.n_triangles; i++) ids[i] = d.triangle_ids ? d.triangle_ids[i] : i;
+    // (copies only when the triangles must be put into leaf order here)
+    std::vector<pcr_triangle> own_tris;
+    std::vector<int32_t> own_ids;
+    const pcr_triangle* tris = d.triangles;
+    const int32_t* ids = d.triangle_ids;
     std::vector<pcr_bvh_node> bvh;
     if (d.n_triangles > 0) {
-        if (d.n_bvh_nodes > 0 && d.bvh_nodes)
+        if (d.n_bvh_nodes > 0 && d.bvh_nodes) {
             bvh.assign(d.bvh_nodes, d.bvh_nodes + d.n_bvh_nodes);
-        else
-            bvh = device_build_bvh(device_, stream_, pool_, tris, &ids);
+        } else {
+            own_tris.assign(d.triangles, d.triangles + d.n_triangles);
+            own_ids.resize(d.n_triangles);
+            for (int i = 0; i < d.n_triangles; i++) own_ids[i] = d.triangle_ids ? d.triangle_ids[i] : i;
+            bvh = device_build_bvh(device_, stream_, pool_, own_tris, &own_ids);
+            tris = own_tris.data();
+            ids = own_ids.data();
+        }
     }
     for (const auto& n : bvh)
         if (n.count == 0 && (n.left_or_first < 0 || n.left_or_first >= (int)bvh.size() || n.right_child < 0 ||
@@ -469,17 +477,21 @@ int Engine::upload_scene(const pcr_scene_desc& d)
         return T;
     };
     int emissive_tris = 0;
-    std::vector<DTri> dtris(d.n_triangles);
-    std::vector<float4> tri_n((size_t)d.n_triangles * 3), tri_flat(d.n_triangles);
     for (int i = 0; i < d.n_triangles; i++) {
         check_mat(tris[i].mat, "triangle");
-        dtris[i] = to_dtri(tris[i], ids[i]);
         if (e.mats[tris[i].mat].flags & kMatEmissive) emissive_tris = 1;
-        tri_n[i * 3 + 0] = make_float4(tris[i].n0[0], tris[i].n0[1], tris[i].n0[2], 0.f);
-        tri_n[i * 3 + 1] = make_float4(tris[i].n1[0], tris[i].n1[1], tris[i].n1[2], 0.f);
-        tri_n[i * 3 + 2] = make_float4(tris[i].n2[0], tris[i].n2[1], tris[i].n2[2], 0.f);
-        tri_flat[i] = make_float4(tris[i].flat_n[0], tris[i].flat_n[1], tris[i].flat_n[2], 0.f);
     }
+    std::vector<DTri> dtris(d.n_triangles);
+    std::vector<float4> tri_n((size_t)d.n_triangles * 3), tri_flat(d.n_triangles);
+    parallel_for(d.n_triangles, [&](int lo, int hi) {
+        for (int i = lo; i < hi; i++) {
+            dtris[i] = to_dtri(tris[i], ids ? ids[i] : i);
+            tri_n[i * 3 + 0] = make_float4(tris[i].n0[0], tris[i].n0[1], tris[i].n0[2], 0.f);
+            tri_n[i * 3 + 1] = make_float4(tris[i].n1[0], tris[i].n1[1], tris[i].n1[2], 0.f);
+            tri_n[i * 3 + 2] = make_float4(tris[i].n2[0], tris[i].n2[1], tris[i].n2[2], 0.f);
+            tri_flat[i] = make_float4(tris[i].flat_n[0], tris[i].flat_n[1], tris[i].flat_n[2], 0.f);
+        }
+    });
     // lights
     std::vector<DLight> lights(d.n_lights);
     int n_lt = 0;

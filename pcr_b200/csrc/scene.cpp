@@ -726,21 +726,32 @@ std::vector<DNode4> collapse_bvh4(const std::vector<pcr_bvh_node>& bvh, int n_tr
         float dx = n.bmax[0] - n.bmin[0], dy = n.bmax[1] - n.bmin[1], dz = n.bmax[2] - n.bmin[2];
         return dx * dy + dy * dz + dz * dx;
     };
-    std::function<int(int)> rec = [&](int b) -> int {
+    out.reserve(bvh.size() / 2 + 1);
+    // depth-first preorder: a 4-wide node takes the next index when it is
+    // reached, its internal children are visited in slot order
+    struct Item { int b, parent, slot; };
+    std::vector<Item> stack{{0, -1, 0}};
+    while (!stack.empty()) {
+        const Item it = stack.back();
+        stack.pop_back();
+        if (out.size() >= bvh.size()) throw PcrError(PCR_ERR_INVALID, "BVH is not a tree");
         const int me = (int)out.size();
         out.emplace_back();
-        std::vector<int> ch;
-        if (bvh[b].count > 0) ch.push_back(b);
-        else { ch.push_back(bvh[b].left_or_first); ch.push_back(bvh[b].right_child); }
-        while (ch.size() < 4) {
+        if (it.parent >= 0) reinterpret_cast<int*>(&out[it.parent].child)[it.slot] = me;
+        int ch[4], nc = 0;
+        if (bvh[it.b].count > 0) ch[nc++] = it.b;
+        else { ch[nc++] = bvh[it.b].left_or_first; ch[nc++] = bvh[it.b].right_child; }
+        while (nc < 4) {   // open the internal child with the largest area
             int pick = -1;
             float best = -1.f;
-            for (size_t k = 0; k < ch.size(); k++)
-                if (bvh[ch[k]].count == 0 && area(ch[k]) > best) { best = area(ch[k]); pick = (int)k; }
+            for (int k = 0; k < nc; k++)
+                if (bvh[ch[k]].count == 0 && area(ch[k]) > best) { best = area(ch[k]); pick = k; }
             if (pick < 0) break;
-            int c = ch[pick];
-            ch.erase(ch.begin() + pick);
-            ch.insert(ch.begin() + pick, {bvh[c].left_or_first, bvh[c].right_child});
+            const int c = ch[pick];
+            for (int k = nc; k > pick + 1; k--) ch[k] = ch[k - 1];
+            ch[pick] = bvh[c].left_or_first;
+            ch[pick + 1] = bvh[c].right_child;
+            nc++;
         }
         float lo[3][4], hi[3][4];
         // empty slots: the code of a leaf with no triangles
@@ -748,7 +759,7 @@ std::vector<DNode4> collapse_bvh4(const std::vector<pcr_bvh_node>& bvh, int n_tr
         int code[4] = {empty, empty, empty, empty}, valid[4] = {0, 0, 0, 0};
         for (int k = 0; k < 4; k++)
             for (int a = 0; a < 3; a++) { lo[a][k] = 0.f; hi[a][k] = 0.f; }
-        for (size_t k = 0; k < ch.size(); k++) {
+        for (int k = 0; k < nc; k++) {
             const pcr_bvh_node& n = bvh[ch[k]];
             for (int a = 0; a < 3; a++) { lo[a][k] = n.bmin[a]; hi[a][k] = n.bmax[a]; }
             valid[k] = 1;
@@ -758,7 +769,7 @@ std::vector<DNode4> collapse_bvh4(const std::vector<pcr_bvh_node>& bvh, int n_tr
                     throw PcrError(PCR_ERR_INVALID, "BVH leaf range out of bounds");
                 code[k] = (int)(0x80000000u | ((uint32_t)n.count << 24) | (uint32_t)n.left_or_first);
             } else {
-                code[k] = rec(ch[k]);
+                code[k] = -1;   // set when the child is reached
             }
         }
         DNode4& N = out[me];
@@ -770,10 +781,21 @@ std::vector<DNode4> collapse_bvh4(const std::vector<pcr_bvh_node>& bvh, int n_tr
         N.hiz = make_float4(hi[2][0], hi[2][1], hi[2][2], hi[2][3]);
         N.child = make_int4(code[0], code[1], code[2], code[3]);
         N.valid = make_int4(valid[0], valid[1], valid[2], valid[3]);
-        return me;
-    };
-    rec(0);
+        for (int k = nc - 1; k >= 0; k--)
+            if (bvh[ch[k]].count == 0) stack.push_back({ch[k], me, k});
+    }
     return out;
+}
+
+void parallel_for(int n, const std::function<void(int, int)>& fn)
+{
+    const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+    const int parts = n < (1 << 16) ? 1 : std::min(16, hw);
+    if (parts <= 1) {
+        if (n > 0) fn(0, n);
+        return;
+    }
+    parallel_chunks(0, n, parts, [&](int, int lo, int hi) { fn(lo, hi); });
 }
 
 // ============================================================ SPD / OBJ

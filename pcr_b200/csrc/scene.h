@@ -6,6 +6,7 @@
 
 #include <cstdint>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,10 @@ std::vector<pcr_bvh_node> build_bvh(std::vector<pcr_triangle>& tris, std::vector
 // Greedy collapse of the binary tree into 4-wide nodes whose child boxes are
 // the binary nodes' boxes verbatim.
 std::vector<DNode4> collapse_bvh4(const std::vector<pcr_bvh_node>& bvh, int n_tris);
+
+// fn(lo, hi) over [0, n) in contiguous ranges on up to 16 host threads
+// (inline below 64K items).
+void parallel_for(int n, const std::function<void(int, int)>& fn);
 
 // RGBToSpectrum::fitSigmoidCoefficients (code/RGBToSpectrum.cpp:256-293).
 void fit_sigmoid(const float rgb[3], const std::vector<float>* lut, float out[4]);
