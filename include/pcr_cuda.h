@@ -105,6 +105,12 @@ typedef struct {
      * to the full image, and pcr_tonemap makes the 8-bit image of the sum.
      * Not with adaptive sampling. */
     int32_t sample_begin, sample_end;
+    /* spectral_fork = false of the GPU backends (code/Includes/GpuDefaults.h:55-71,
+     * code/Gpu/Metal/MetalRenderer.mm:2155-2252): at the first dispersive
+     * refraction a path keeps its hero wavelength alone, scaled by the number
+     * of hero wavelengths, instead of forking one sub-path per wavelength.
+     * 0 = fork (default, as the CPU renderer). */
+    int32_t spectral_terminate;
 } pcr_render_desc;
 
 typedef struct {

@@ -89,7 +89,8 @@ class RenderDesc(C.Structure):
         "stratified", "aa_samples", "adaptive", "aces", "denoise")] + [("seed", C.c_uint64), ("priority", C.c_int32),
                                                                 ("multi_sample", C.c_int32),
                                                                 ("sample_begin", C.c_int32),
-                                                                ("sample_end", C.c_int32)]
+                                                                ("sample_end", C.c_int32),
+                                                                ("spectral_terminate", C.c_int32)]
 
 
 class RenderStats(C.Structure):
@@ -193,10 +194,10 @@ def _ip(a):
 
 def render_desc(width, height=None, depth=4, samples=16, shadow=4, spectral=True, hero=4, mis=False,
                 russian=False, stratified=False, aa=1, adaptive=False, aces=False, denoise=False, seed=1,
-                priority=0, multi_sample=False, sample_begin=0, sample_end=0) -> RenderDesc:
+                priority=0, multi_sample=False, sample_begin=0, sample_end=0, terminate=False) -> RenderDesc:
     return RenderDesc(width, height or width, depth, samples, shadow, int(spectral), hero, int(mis),
                       int(russian), int(stratified), aa, int(adaptive), int(aces), int(denoise), seed, priority,
-                      int(multi_sample), sample_begin, sample_end)
+                      int(multi_sample), sample_begin, sample_end, int(terminate))
 
 
 class HostScene:

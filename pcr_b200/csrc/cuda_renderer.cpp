@@ -124,6 +124,7 @@ pcr_render_desc CudaRenderer::desc() const
     d.aces = useACES;
     d.denoise = useDenoise;
     d.multi_sample = wavefrontMultiSample;
+    d.spectral_terminate = spectralFork ? 0 : 1;
     d.seed = seed ? seed : (uint64_t)std::random_device{}() << 32 | std::random_device{}();
     return d;
 }

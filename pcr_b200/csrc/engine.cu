@@ -757,7 +757,7 @@ void Engine::activate(Request& r, int slot)
     R.paths_per_pixel = R.aa * R.local_spp;
     R.shadow = d.shadow_samples;
     R.flags = (d.spectral ? kReqSpectral : 0) | (d.mis ? kReqMIS : 0) | (d.russian ? kReqRussian : 0) |
-              (d.stratified ? kReqStratified : 0);
+              (d.stratified ? kReqStratified : 0) | (d.spectral_terminate ? kReqTerminate : 0);
     R.hero = std::min(4, std::max(1, d.hero_samples <= 0 ? 4 : d.hero_samples));
     R.strata = d.stratified ? std::max(1, (int)std::lround(std::sqrt((float)d.samples))) : 0;
     R.cam_x = S.cam[0];
@@ -1378,7 +1378,7 @@ DRequest Engine::make_request(const pcr_render_desc& d, int scene, double* accum
     R.paths_per_pixel = R.aa * R.local_spp;
     R.shadow = d.shadow_samples;
     R.flags = (d.spectral ? kReqSpectral : 0) | (d.mis ? kReqMIS : 0) | (d.russian ? kReqRussian : 0) |
-              (d.stratified ? kReqStratified : 0);
+              (d.stratified ? kReqStratified : 0) | (d.spectral_terminate ? kReqTerminate : 0);
     R.hero = std::min(4, std::max(1, d.hero_samples <= 0 ? 4 : d.hero_samples));
     R.strata = d.stratified ? std::max(1, (int)std::lround(std::sqrt((float)d.samples))) : 0;
     R.cam_x = S.cam[0];

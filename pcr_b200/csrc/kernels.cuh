@@ -453,6 +453,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
         int forked = 0;       // sub-paths written by a dispersive fork
         float3 no = make_float3(0, 0, 0), nd = no;
         float4 ntp = make_float4(0, 0, 0, 0);
+        bool term = false;    // continues with its hero wavelength alone
         double* acc = nullptr;
         float3 emit_xyz = make_float3(0, 0, 0);
         bool emit = false;
@@ -567,7 +568,12 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
             } else if (m.flags & kMatTransparent) {
                 if (!last) {
                     const float cosI = -f3dot(d, N);
-                    const bool disperse = spectral && m.cauchyB != 0.f && !single && nHero > 1;
+                    const bool dispersive = spectral && m.cauchyB != 0.f && !single && nHero > 1;
+                    // fork: one sub-path per wavelength (code/Renderer.cpp:736-753);
+                    // terminate: the hero wavelength's bounce alone
+                    // (code/Gpu/Metal/MetalRenderer.mm:2143-2252)
+                    const bool terminate = dispersive && (R.flags & kReqTerminate);
+                    const bool disperse = dispersive && !terminate;
                     const int ways = disperse ? nHero : 1;
                     const float4 coins = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce, 63u);
                     const float4 alg = spectral ? spec4(m, 0, lam4) : rgb4(m.albedo);
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                     for (int k = 0; k < ways; k++) {
                         const float lk = comp4(lam4, k);
                         float ior = m.ior;
-                        if (spectral && m.cauchyB != 0.f && (disperse || single))
+                        if (spectral && m.cauchyB != 0.f && (dispersive || single))
                             ior = m.ior + m.cauchyB * 1e4f / (lk * lk);  // Optics::cauchyIor
                         // Optics::dielectricBounce (code/Includes/Optics.h:59-82)
                         const float n1 = entering ? 1.f : ior, n2 = entering ? ior : 1.f;
@@ -627,10 +633,19 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         } else {
                             no = bo;
                             nd = bd;
+                            // a refraction ends the other wavelengths; the
+                            // hero's share is scaled by their number so the
+                            // estimate stays unbiased (a reflection does not
+                            // depend on the wavelength and keeps them all)
+                            term = terminate && !refl;
                         }
                     }
                     if (!disperse) {
                         ntp = mul4(tp4, alg);
+                        if (term) {
+                            const float h0 = ntp.x * (float)nHero;
+                            ntp = make_float4(h0, h0, h0, h0);
+                        }
                         cont = true;
                     }
                 }
@@ -757,7 +772,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
         // ---- emit work (block-uniform control flow from here)
         if (emit) add_xyz(acc, emit_xyz);
         {
-            const int newMeta = (bounce + 1) | (fork << 8) | (single << 11) | (nHero << 12);
+            const int newMeta = (bounce + 1) | (fork << 8) | ((single | (term ? 1 : 0)) << 11) | (nHero << 12);
             // one contiguous range per block (its warps in order), so the
             // next launch's warps rarely straddle two blocks' outputs, which
             // may belong to different scenes
@@ -781,9 +796,10 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                 NQ.tp[pos] = ntp;
                 NQ.id[pos] = id;
                 if (spec_path) {
-                    NQ.w[0][pos] = Q.w[0][i];
-                    NQ.w[1][pos] = Q.w[1][i];
-                    NQ.w[2][pos] = Q.w[2][i];
+                    const float4 w0 = Q.w[0][i];
+                    NQ.w[0][pos] = term ? make_float4(w0.x, w0.y, w0.z, 0.f) : w0;
+                    NQ.w[1][pos] = term ? make_float4(0.f, 0.f, 0.f, 0.f) : Q.w[1][i];
+                    NQ.w[2][pos] = term ? make_float4(0.f, 0.f, 0.f, 0.f) : Q.w[2][i];
                 }
             }
         }

@@ -110,7 +110,8 @@ struct DScene {
 };
 
 // Request flags
-constexpr int kReqSpectral = 1, kReqMIS = 2, kReqRussian = 4, kReqStratified = 8, kReqAdaptive = 16;
+constexpr int kReqSpectral = 1, kReqMIS = 2, kReqRussian = 4, kReqStratified = 8, kReqAdaptive = 16,
+              kReqTerminate = 32;
 
 struct DRequest {
     int scene, width, height, depth;

@@ -194,3 +194,29 @@ def test_many_shadow_samples_grow_the_shadow_queue(ctx):
     with pytest.raises(capi.PcrError):
         ctx.render(sid, capi.render_desc(16, samples=1, shadow=65))
     ctx.release_scene(sid)
+
+
+def test_spectral_terminate_keeps_the_mean_and_traces_fewer_rays(ctx):
+    """spectral_terminate (the GPU backends' spectralFork = false): at a
+    dispersive refraction a path keeps its hero wavelength alone, scaled by
+    the number of hero wavelengths.  It estimates the same image as the
+    4-way fork with fewer rays, and is inert where no glass disperses."""
+    from pcr_b200 import capi
+    sid = ctx.load_scene_json(scene_path("cornell-glass"), GOLDEN)
+    means, rays = [], []
+    for term in (False, True):
+        ctx.reset_stats()
+        img = ctx.render(sid, capi.render_desc(48, depth=6, samples=512, shadow=2, seed=17,
+                                               terminate=term))[0].astype(np.float64)
+        rays.append(ctx.stats()["rays"])
+        means.append(img.reshape(-1, 3).mean(0))
+    # ~1.2M paths per image: the two unbiased estimates agree to a few tenths
+    # of a percent; 2 % leaves room for the noisier caustic
+    assert np.all(np.abs(means[1] - means[0]) <= 0.02 * np.abs(means[0])), means
+    assert rays[1] < rays[0], rays
+    ctx.release_scene(sid)
+    sid = ctx.load_scene_json(scene_path("cornell"), GOLDEN)
+    a = ctx.render(sid, capi.render_desc(32, depth=4, samples=8, shadow=2, seed=3))
+    b = ctx.render(sid, capi.render_desc(32, depth=4, samples=8, shadow=2, seed=3, terminate=True))
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+    ctx.release_scene(sid)
