@@ -70,3 +70,26 @@ def test_cli_denoise_adaptive_aces_match_library(tmp_path):
                                                      denoise=True, aa=6, adaptive=True, aces=True))
     ctx.close()
     assert np.array_equal(rgb, lib_rgb)
+
+
+@pytest.mark.parametrize("terminate", [False, True])
+def test_cli_spectral_terminate_matches_library(tmp_path, terminate):
+    """--spectral-terminate sets CudaRenderer::spectralFork = false, which
+    reaches the device as spectral_terminate; the default forks."""
+    from PIL import Image
+    from pcr_b200 import capi
+    args = [CLI, "--scenes-dir", os.path.join(GOLDEN, "scenes"), "--scene", "cornell-glass", "-w", "40",
+            "--height", "40", "-d", "5", "-s", "16", "-S", "2", "--spectral", "--seed", "9", "-o", str(tmp_path)]
+    if terminate:
+        args.append("--spectral-terminate")
+    out = subprocess.run(args, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    files = os.listdir(tmp_path)
+    rgb = np.asarray(Image.open(tmp_path / files[0]).convert("RGB"))
+    ctx = capi.Context()
+    sid = ctx.load_scene_json(scene_path("cornell-glass"), GOLDEN)
+    lib = [ctx.render(sid, capi.render_desc(40, 40, depth=5, samples=16, shadow=2, spectral=True, seed=9,
+                                            terminate=t))[1] for t in (False, True)]
+    ctx.close()
+    assert np.array_equal(rgb, lib[int(terminate)])
+    assert not np.array_equal(lib[0], lib[1])
