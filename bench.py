@@ -47,6 +47,15 @@ HBM_FALLBACK = 6650.0
 # command are kept in the profiles directory).  Traffic grows in proportion to
 # the units, so a launch's traffic is this figure times its units.
 NCU_DRAM_PER_UNIT = {"extend": 48.8, "shade": 409.3, "shadow": 67.6}
+# Issue-rate side of the same kernels (ncu --set full, one launch each of an
+# 8-render batch, summarised in the profiles directory): the share of issue
+# slots used (sm__inst_issued over the schedulers' cycles) and the share of
+# a warp's 32 lanes active per instruction.  The plane and triangle tests are
+# dependent IEEE-exact FP32 chains, so these kernels are bound by issue and
+# latency rather than by DRAM.
+NCU_ISSUE = {"extend": {"issue_slots_busy": 0.674, "lanes_active": 14.8 / 32},
+             "shade": {"issue_slots_busy": 0.323, "lanes_active": 23.1 / 32},
+             "shadow": {"issue_slots_busy": 0.526, "lanes_active": 21.4 / 32}}
 
 
 def args_():
@@ -460,6 +469,7 @@ def main():
                     "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
                     "traffic_note": "ncu DRAM bytes per unit (8-render capture) x units per launch",
                     "bytes_per_launch": bytes_stage[dom] / n_l, "ms_per_launch": t_ms / n_l,
+                    "issue": dict(NCU_ISSUE.get(dom, {}), note="ncu, one launch per kernel of an 8-render batch"),
                     "stage_ms": ps["stage_ms"], "stage_share": {k: v / max(1e-9, sum(ps["stage_ms"].values()))
                                                                 for k, v in ps["stage_ms"].items()}}
 
