@@ -65,13 +65,23 @@ __device__ __forceinline__ bool sphere_hit(const DSphere& s, float3 o, float3 d,
     return true;
 }
 
+// One-instruction reciprocal (PTX rcp.approx.ftz.f32) for conservative
+// pre-filters only; never for a value the reference computes.
+__device__ __forceinline__ float rcp_approx(float x)
+{
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // Plane::intersect (code/Includes/Plane.h:33-54); uu, vv precomputed with
 // the same dot the reference evaluates per call.
 //
 // The three IEEE divides are first decided by a reciprocal product: for
-// x > 0, y > 0 normal, x * rcp(y) is within 2^-23 relative of x / y, so a
-// product beyond a bound by 2^-20 fixes the comparison the correctly rounded
-// quotient would make.  Only the t of planes that survive, and quotients near
+// x > 0, y > 0 normal, x * rcp_approx(y) is within 2^-21 relative of x / y
+// (the instruction's reciprocal is within 2 ulp, the product adds half an
+// ulp), so a product beyond a bound by 2^-20 fixes the comparison the
+// correctly rounded quotient would make.  Only the t of planes that survive, and quotients near
 // a bound, are divided exactly; the accept/reject decisions and t are the
 // same as dividing every time.  t0 is only meaningful when true is returned.
 __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, float closest, float& t0)
@@ -88,7 +98,7 @@ __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, f
     // t = num / denom is <= 0 when the signs differ (or num is zero)
     const float an = denom > 0.f ? num : -num;
     if (an <= 0.f) return false;
-    const float tq = an * __frcp_rn(fabsf(denom));
+    const float tq = an * rcp_approx(fabsf(denom));
     if (tq > closest * kUp || tq < 1e-6f * kDown) return false;
     float t = div(num, denom);
     t0 = t;
@@ -103,7 +113,7 @@ __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, f
     // makes s negative (|a / uu| stays far above the smallest subnormal for
     // any |u| < 1e12).
     if (a < -1e-20f || b < -1e-20f) return false;
-    if (a * __frcp_rn(u.w) > kUp || b * __frcp_rn(v.w) > kUp) return false;
+    if (a * rcp_approx(u.w) > kUp || b * rcp_approx(v.w) > kUp) return false;
     float s = div(a, u.w);
     float q = div(b, v.w);
     if (s > 1.f || s < 0.f || q > 1.f || q < 0.f) return false;
