@@ -129,14 +129,32 @@ __device__ __forceinline__ bool tri_hit(float4 a, float4 b, float4 c, float3 o, 
     float3 pvec = cross(d, e2);
     float det = dot(e1, pvec);
     if (fabsf(det) < 1e-6f) return false;
-    float invDet = div(1.f, det);
+    // Clear rejections are decided before the exact reciprocal: with
+    // r = rcp_approx(det), x * r is within 2^-21 relative of x * (1 / det),
+    // so a product below -1e-30 (far from underflow) is negative in the
+    // exact arithmetic too, and one beyond a bound by 2^-20 (2^-19 for the
+    // sum of two) is beyond it there.  Triangles that pass run the
+    // reference's arithmetic unchanged.
+    const float kUp = 1.f + 9.5367431640625e-07f, kUp2 = 1.f + 1.9073486328125e-06f;
+    const float kDown = 1.f - 9.5367431640625e-07f;
+    const float r = rcp_approx(det);
     float3 tvec = sub3(o, v0);
-    float u = mul(dot(tvec, pvec), invDet);
-    if (u < 0.f || u > 1.f) return false;
+    const float U = dot(tvec, pvec);
+    const float ua = U * r;
+    if (ua < -1e-30f || ua > kUp) return false;
     float3 qvec = cross(tvec, e1);
-    float v = mul(dot(d, qvec), invDet);
+    const float V = dot(d, qvec);
+    const float va = V * r;
+    if (va < -1e-30f || ua + va > kUp2) return false;
+    const float T = dot(e2, qvec);
+    const float ta = T * r;
+    if (ta < 1e-6f * kDown || ta > closest * kUp) return false;
+    float invDet = div(1.f, det);
+    float u = mul(U, invDet);
+    if (u < 0.f || u > 1.f) return false;
+    float v = mul(V, invDet);
     if (v < 0.f || add(u, v) > 1.f) return false;
-    float t = mul(dot(e2, qvec), invDet);
+    float t = mul(T, invDet);
     if (t <= 1e-6f || t >= closest) return false;
     t_out = t;
     u_out = u;
@@ -272,8 +290,9 @@ __device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d,
 // Conservative ray-box test for a plane group.  The box is padded on the
 // host by well over the rounding error of a hit point, the segment end by
 // 1e-4 relative; direction components below 1e-30 count as zero (the ray
-// then moves less than the padding along that axis).  A false answer means
-// no plane of the group can be hit in (0, closest].
+// then moves less than the padding along that axis), the others enter as
+// their 1-ulp rcp_approx, whose error the padding also covers.  A false
+// answer means no plane of the group can be hit in (0, closest].
 __device__ __forceinline__ bool group_axis(float lo, float hi, float o, float d, float r, float& tmin, float& tmax)
 {
     if (fabsf(d) < 1e-30f) return o >= lo && o <= hi;
@@ -309,7 +328,7 @@ __device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, flo
     // planes in order, a group's planes skipped together when the ray cannot
     // reach the group's (padded) box before `closest`; skipping planes that
     // cannot be hit leaves the closest hit and its tie order unchanged
-    const float3 rd = make_float3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    const float3 rd = make_float3(rcp_approx(d.x), rcp_approx(d.y), rcp_approx(d.z));
     for (int g = 0; g < S.n_pgroups; g++) {
         const float4 lo = S.pgroups[2 * g], hi = S.pgroups[2 * g + 1];
         const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
@@ -371,7 +390,7 @@ __device__ __forceinline__ bool scene_blocked(const DScene& S, const DMaterial* 
             bound = t0;
         }
     }
-    const float3 rd = make_float3(__frcp_rn(d.x), __frcp_rn(d.y), __frcp_rn(d.z));
+    const float3 rd = make_float3(rcp_approx(d.x), rcp_approx(d.y), rcp_approx(d.z));
     for (int g = 0; g < S.n_sgroups; g++) {
         const float4 lo = S.sgroups[2 * g], hi = S.sgroups[2 * g + 1];
         const int first = __float_as_int(lo.w), count = __float_as_int(hi.w);
