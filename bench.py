@@ -46,16 +46,16 @@ HBM_FALLBACK = 6650.0
 # 8-render step, divided by that step's rays / shadow rays; the summary and
 # command are kept in the profiles directory).  Traffic grows in proportion to
 # the units, so a launch's traffic is this figure times its units.
-NCU_DRAM_PER_UNIT = {"extend": 48.8, "shade": 409.3, "shadow": 67.6}
+NCU_DRAM_PER_UNIT = {"extend": 48.5, "shade": 408.4, "shadow": 67.6}
 # Issue-rate side of the same kernels (ncu --set full, one launch each of an
 # 8-render batch, summarised in the profiles directory): the share of issue
 # slots used (sm__inst_issued over the schedulers' cycles) and the share of
 # a warp's 32 lanes active per instruction.  The plane and triangle tests are
 # dependent IEEE-exact FP32 chains, so these kernels are bound by issue and
 # latency rather than by DRAM.
-NCU_ISSUE = {"extend": {"issue_slots_busy": 0.674, "lanes_active": 14.8 / 32},
-             "shade": {"issue_slots_busy": 0.323, "lanes_active": 23.1 / 32},
-             "shadow": {"issue_slots_busy": 0.526, "lanes_active": 21.4 / 32}}
+NCU_ISSUE = {"extend": {"issue_slots_busy": 0.658, "lanes_active": 15.5 / 32},
+             "shade": {"issue_slots_busy": 0.324, "lanes_active": 23.1 / 32},
+             "shadow": {"issue_slots_busy": 0.480, "lanes_active": 21.8 / 32, "l1_busy": 0.81}}
 
 
 def args_():
