@@ -76,6 +76,8 @@ def args_():
                    help="skip the autotuner (queue size, block size, issue chunk, refill cadence)")
     p.add_argument("--serve-requests", type=int, default=2000, help="served stream length (2000: the serving config)")
     p.add_argument("--serve-rate", type=float, default=200.0)
+    p.add_argument("--serve-scale", type=int, default=0,
+                   help="serving at scale: requests per stream (0: off; the 1M-triangle mesh is generated on first use)")
     return p.parse_args()
 
 
@@ -332,6 +334,64 @@ def serve_run(ctx, sids, files, data, a, n=None, rate=None, seed_off=17):
             "mesh_fraction": 0.2, "resolution": "log-uniform 64..1024"}
 
 
+def serve_scale_run(ctx, sids, data, a):
+    """Serving at scale: 10 % heavy requests (2048x2048, depth 8, 64 paths
+    per pixel, 4 shadow rays) over the seeded 1,003,520-triangle displaced
+    icosphere, 90 % small ones (square 64..256, the served stream's scene
+    mix: the 10 variants and 20 % the ~70k-triangle mesh).  A closed-loop
+    pass (every request submitted at once) measures the saturation rate; the
+    reported stream then arrives by a Poisson process at 80 % of it."""
+    from pcr_b200 import capi, workloads
+    mesh = {False: ctx.load_scene_json(workloads.mesh_scene(59, 11, glass=False), data),
+            True: ctx.load_scene_json(workloads.mesh_scene(59, 12, glass=True), data)}
+    path = workloads.mesh_scene(224, 1)
+    t0 = time.perf_counter()
+    big = ctx.load_scene_json(path, data)
+    load_s = time.perf_counter() - t0
+    heavy = {"variant": "mesh1m", "width": 2048, "height": 2048, "depth": 8, "samples": 64, "shadow": 4}
+
+    def run(reqs):
+        ctx.serve_start()
+        t0 = time.perf_counter()
+        ids = []
+        for r in reqs:
+            now = time.perf_counter() - t0
+            if r["arrival"] > now:
+                time.sleep(r["arrival"] - now)
+            sid = (big if r["variant"] == "mesh1m" else
+                   mesh[bool(r["seed"] & 1)] if r["variant"] == "mesh" else sids[r["variant"]])
+            d = capi.render_desc(r["width"], r["height"], depth=r["depth"], samples=r["samples"],
+                                 shadow=r["shadow"], spectral=True, seed=r["seed"])
+            ids.append((ctx.submit(sid, d), r))
+        lat, hv, paths, t_last = [], [], 0, 0.0
+        for rid, r in ids:
+            ctx.wait(rid, 600_000)
+            _, _, st = ctx.fetch(rid, want_hdr=False, want_rgb=False)
+            lat.append(st.latency_ms)
+            hv.append(r["variant"] == "mesh1m")
+            paths += st.paths
+            t_last = max(t_last, r["arrival"] * 1e3 + st.latency_ms)
+        ctx.serve_stop()
+        return np.asarray(lat), np.asarray(hv), paths, t_last / 1e3
+
+    n = a.serve_scale
+    mix = dict(res=(64, 256), mesh_fraction=0.2, heavy_fraction=0.1, heavy=heavy)
+    _, _, sat_paths, sat_span = run(workloads.request_stream(n, 1e9, seed=a.seed + 41, **mix))
+    sat_rate = n / sat_span
+    reqs = workloads.request_stream(n, 0.8 * sat_rate, seed=a.seed + 43, **mix)
+    lat, hv, paths, span = run(reqs)
+
+    def pct(x, q):
+        return float(np.percentile(x, q)) if x.size else None
+    return {"requests": n, "heavy": int(hv.sum()), "saturation_req_s": sat_rate,
+            "saturation_paths_per_s": sat_paths / sat_span, "rate_req_s": 0.8 * sat_rate,
+            "p50_ms": pct(lat, 50), "p99_ms": pct(lat, 99), "max_ms": float(lat.max()),
+            "small_p50_ms": pct(lat[~hv], 50), "small_p99_ms": pct(lat[~hv], 99),
+            "heavy_p50_ms": pct(lat[hv], 50), "heavy_p99_ms": pct(lat[hv], 99),
+            "paths_per_s": paths / span, "span_s": span, "mesh_1m_load_s": load_s,
+            "mix": "10 % 2048x2048 d8 s64 S4 on 1,003,520 triangles; 90 % 64..256 squares"}
+
+
 # ------------------------------------------------------------------ CUDA arm
 def main():
     a = args_()
@@ -484,6 +544,8 @@ def main():
         serve["at_80pct_capacity"] = serve_run(ctx, sids, files, data, a, n=min(400, a.serve_requests),
                                                rate=0.8 * cap, seed_off=29)
 
+    serve_scale = serve_scale_run(ctx, sids, data, a) if a.serve_scale > 0 else None
+
     # ---- Cornell configuration at matched image error
     matched = None
     if not a.no_matched:
@@ -521,7 +583,7 @@ def main():
             "plain_value": plain, "batched_over_plain": (value / plain) if plain else None,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
-            "serve": serve, "matched_rmse": matched,
+            "serve": serve, "serve_scale": serve_scale, "matched_rmse": matched,
             "tuning": {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")},
             "autotune": autotune,
         }
