@@ -76,6 +76,8 @@ def args_():
                    help="skip the autotuner (queue size, block size, issue chunk, refill cadence)")
     p.add_argument("--serve-requests", type=int, default=2000, help="served stream length (2000: the serving config)")
     p.add_argument("--serve-rate", type=float, default=200.0)
+    p.add_argument("--mesh-batch", type=int, default=0,
+                   help="batched mesh scenes: renders per step (0: off; 32 = the mesh configuration)")
     p.add_argument("--serve-scale", type=int, default=0,
                    help="serving at scale: requests per stream (0: off; the 1M-triangle mesh is generated on first use)")
     return p.parse_args()
@@ -392,6 +394,44 @@ def serve_scale_run(ctx, sids, data, a):
             "mix": "10 % 2048x2048 d8 s64 S4 on 1,003,520 triangles; 90 % 64..256 squares"}
 
 
+def mesh_batch_run(ctx, stream, data, a):
+    """Batched mesh scenes: the Cornell box with the seeded ~70k-triangle
+    displaced icosphere, glass or Lambertian by seed (50/50); `n` renders
+    per step, square resolution log-uniform 512..1024, depth 8, 32 paths per
+    pixel, 4 shadow rays.  Device-timed like the main batched value (one
+    warm-up step, then `a.steps` steps)."""
+    import torch
+
+    from pcr_b200 import capi, workloads
+    sids = {g: ctx.load_scene_json(workloads.mesh_scene(59, 21 + int(g), glass=g), data) for g in (False, True)}
+    rng = np.random.default_rng(a.seed + 53)
+    batch = []
+    for _ in range(a.mesh_batch):
+        side = int(round(np.exp(rng.uniform(np.log(512), np.log(1024)))))
+        batch.append((sids[bool(rng.integers(0, 2))], capi.render_desc(side, depth=8, samples=32, shadow=4,
+                                                                       spectral=True, seed=int(rng.integers(1, 2**31)))))
+    paths = sum(d.width * d.height * d.samples for _, d in batch)
+
+    def step():
+        ids = [ctx.submit(s, d) for s, d in batch]
+        ctx.run_until_idle()
+        for i in ids:
+            ctx.fetch(i, want_hdr=False, want_rgb=False)
+    step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(a.steps):
+        step()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    s = ev0.elapsed_time(ev1) / 1e3
+    for v in sids.values():
+        ctx.release_scene(v)
+    return {"renders": a.mesh_batch, "paths_per_step": paths, "paths_per_s": paths * a.steps / s,
+            "ms_per_step": s * 1e3 / a.steps, "triangles": 69620,
+            "config": "512..1024 squares, depth 8, 32 paths per pixel, S 4, glass / Lambertian 50/50"}
+
+
 # ------------------------------------------------------------------ CUDA arm
 def main():
     a = args_()
@@ -545,6 +585,7 @@ def main():
                                                rate=0.8 * cap, seed_off=29)
 
     serve_scale = serve_scale_run(ctx, sids, data, a) if a.serve_scale > 0 else None
+    mesh_batch = mesh_batch_run(ctx, stream, data, a) if a.mesh_batch > 0 else None
 
     # ---- Cornell configuration at matched image error
     matched = None
@@ -583,7 +624,7 @@ def main():
             "plain_value": plain, "batched_over_plain": (value / plain) if plain else None,
             "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
-            "serve": serve, "serve_scale": serve_scale, "matched_rmse": matched,
+            "serve": serve, "serve_scale": serve_scale, "mesh_batch": mesh_batch, "matched_rmse": matched,
             "tuning": {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")},
             "autotune": autotune,
         }
