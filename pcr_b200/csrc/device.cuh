@@ -245,20 +245,45 @@ __device__ __forceinline__ int bvh4_closest(const DScene& S, float3 o, float3 d,
                 float t2 = ch.z != kEmpty ? slab4(lx.z, hx.z, ly.z, hy.z, lz.z, hz.z, o, inv, closest) : inf;
                 float t3 = ch.w != kEmpty ? slab4(lx.w, hx.w, ly.w, hy.w, lz.w, hz.w, o, inv, closest) : inf;
                 int c0 = ch.x, c1 = ch.y, c2 = ch.z, c3 = ch.w;
-                // ascending by tNear; misses (+inf) last
-                cas(t0, c0, t1, c1);
-                cas(t2, c2, t3, c3);
-                cas(t0, c0, t2, c2);
-                cas(t1, c1, t3, c3);
-                cas(t1, c1, t2, c2);
                 const int k = (t0 < inf) + (t1 < inf) + (t2 < inf) + (t3 < inf);
                 // the reference skips all children when they would overflow its stack
                 if (k > 0 && top + k - 1 <= kStackSize) {
-                    if (k > 3) { stk[top] = c3; stt[top] = t3; top++; }
-                    if (k > 2) { stk[top] = c2; stt[top] = t2; top++; }
-                    if (k > 1) { stk[top] = c1; stt[top] = t1; top++; }
-                    code = c0;
-                    tcode = t0;
+                    if constexpr (kAny) {
+                        // A shadow query's answer does not depend on the
+                        // visit order (blocked iff some hit in front of the
+                        // bound blocks, and blocking is monotone in t): the
+                        // first hit child in slot order is visited next, the
+                        // others are pushed unsorted.
+                        bool have = false;
+                        auto take = [&](int c, float t) {
+                            if (!(t < inf)) return;
+                            if (!have) {
+                                code = c;
+                                tcode = t;
+                                have = true;
+                            } else {
+                                stk[top] = c;
+                                stt[top] = t;
+                                top++;
+                            }
+                        };
+                        take(c0, t0);
+                        take(c1, t1);
+                        take(c2, t2);
+                        take(c3, t3);
+                    } else {
+                        // ascending by tNear; misses (+inf) last
+                        cas(t0, c0, t1, c1);
+                        cas(t2, c2, t3, c3);
+                        cas(t0, c0, t2, c2);
+                        cas(t1, c1, t3, c3);
+                        cas(t1, c1, t2, c2);
+                        if (k > 3) { stk[top] = c3; stt[top] = t3; top++; }
+                        if (k > 2) { stk[top] = c2; stt[top] = t2; top++; }
+                        if (k > 1) { stk[top] = c1; stt[top] = t1; top++; }
+                        code = c0;
+                        tcode = t0;
+                    }
                     continue;
                 }
             } else {
