@@ -38,6 +38,7 @@
 
 #include "bvh_build.h"
 #include "engine.h"
+#include "scene.h"
 
 namespace pcr {
 namespace {
@@ -864,21 +865,25 @@ std::vector<pcr_bvh_node> device_build_bvh(int device, cudaStream_t st, cudaMemP
     std::vector<int32_t> order;
     const int n = (int)tris.size();
     std::vector<float> v((size_t)n * 9);
-    for (int i = 0; i < n; i++)
-        for (int a = 0; a < 3; a++) {
-            v[(size_t)i * 9 + a] = tris[i].v0[a];
-            v[(size_t)i * 9 + 3 + a] = tris[i].v1[a];
-            v[(size_t)i * 9 + 6 + a] = tris[i].v2[a];
-        }
+    parallel_for(n, [&](int lo, int hi) {
+        for (int i = lo; i < hi; i++)
+            for (int a = 0; a < 3; a++) {
+                v[(size_t)i * 9 + a] = tris[i].v0[a];
+                v[(size_t)i * 9 + 3 + a] = tris[i].v1[a];
+                v[(size_t)i * 9 + 6 + a] = tris[i].v2[a];
+            }
+    });
     device_build_bvh_raw(device, st, pool, v.data(), n, nodes, order);
     std::vector<pcr_triangle> t2(tris.size());
-    for (int i = 0; i < n; i++) t2[i] = tris[order[i]];
+    std::vector<int32_t> i2(ids ? ids->size() : 0);
+    parallel_for(n, [&](int lo, int hi) {
+        for (int i = lo; i < hi; i++) {
+            t2[i] = tris[order[i]];
+            if (ids) i2[i] = (*ids)[order[i]];
+        }
+    });
     tris.swap(t2);
-    if (ids) {
-        std::vector<int32_t> i2(ids->size());
-        for (int i = 0; i < n; i++) i2[i] = (*ids)[order[i]];
-        ids->swap(i2);
-    }
+    if (ids) ids->swap(i2);
     return nodes;
 }
 

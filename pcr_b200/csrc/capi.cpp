@@ -90,10 +90,12 @@ void device_bvh(pcr::Engine& e, pcr::HostScene& s)
     e.build_bvh(s.triangles.data(), n, s.bvh, order);
     std::vector<pcr_triangle> t(n);
     std::vector<int32_t> ids(n);
-    for (int i = 0; i < n; i++) {
-        t[i] = s.triangles[order[i]];
-        ids[i] = s.triangle_ids[order[i]];
-    }
+    pcr::parallel_for(n, [&](int lo, int hi) {
+        for (int i = lo; i < hi; i++) {
+            t[i] = s.triangles[order[i]];
+            ids[i] = s.triangle_ids[order[i]];
+        }
+    });
     s.triangles.swap(t);
     s.triangle_ids.swap(ids);
 }

@@ -1601,12 +1601,14 @@ void Engine::build_bvh(const pcr_triangle* tris, int n, std::vector<pcr_bvh_node
 {
     std::lock_guard<std::mutex> g(run_mu_);
     std::vector<float> v((size_t)n * 9);
-    for (int i = 0; i < n; i++)
-        for (int a = 0; a < 3; a++) {
-            v[(size_t)i * 9 + a] = tris[i].v0[a];
-            v[(size_t)i * 9 + 3 + a] = tris[i].v1[a];
-            v[(size_t)i * 9 + 6 + a] = tris[i].v2[a];
-        }
+    parallel_for(n, [&](int lo, int hi) {
+        for (int i = lo; i < hi; i++)
+            for (int a = 0; a < 3; a++) {
+                v[(size_t)i * 9 + a] = tris[i].v0[a];
+                v[(size_t)i * 9 + 3 + a] = tris[i].v1[a];
+                v[(size_t)i * 9 + 6 + a] = tris[i].v2[a];
+            }
+    });
     device_build_bvh_raw(device_, stream_, pool_, v.data(), n, nodes, order);
 }
 
