@@ -131,3 +131,22 @@ def test_scene_load_builds_on_the_device_with_the_same_hits(ctx):
     ctx.release_scene(sid_dev)
     ctx.release_scene(sid_host)
     hs.close()
+
+
+def test_bvh_build_entry_point_errors(ctx):
+    """pcr_bvh_build: too small an output array is an argument error, an
+    empty input gives no nodes, and the context stays usable after both."""
+    import ctypes as C
+
+    from pcr_b200 import capi
+    tris = np.zeros((100, 23), np.float32)
+    tris[:, :9] = _soup(100, 3)
+    nodes = np.zeros((4, 9), np.float32)
+    order = np.zeros(100, np.int32)
+    m = C.c_int32(0)
+    st = ctx.L.pcr_bvh_build(ctx.h, capi._fp(tris), 100, capi._fp(nodes), 4, C.byref(m), capi._ip(order))
+    assert st == 1 and b"too small" in ctx.L.pcr_last_error()
+    st = ctx.L.pcr_bvh_build(ctx.h, None, 0, None, 0, C.byref(m), None)
+    assert st == 0 and m.value == 0
+    n2, o2 = ctx.build_bvh(_soup(100, 3))
+    _same(n2, o2, *_oracle(_soup(100, 3)))
