@@ -53,6 +53,10 @@ NCU_DRAM_PER_UNIT = {"extend": 48.5, "shade": 408.4, "shadow": 67.6}
 # a warp's 32 lanes active per instruction.  The plane and triangle tests are
 # dependent IEEE-exact FP32 chains, so these kernels are bound by issue and
 # latency rather than by DRAM.
+# Warp instructions per unit (smsp__inst_executed.sum over every launch of
+# one 8-render step, divided by that step's rays / shadow rays), for the
+# issue-rate roofline below.
+NCU_INST_PER_UNIT = {"extend": 42.36, "shade": 54.61, "shadow": 31.57}
 NCU_ISSUE = {"extend": {"issue_slots_busy": 0.658, "lanes_active": 15.5 / 32},
              "shade": {"issue_slots_busy": 0.324, "lanes_active": 23.1 / 32},
              "shadow": {"issue_slots_busy": 0.480, "lanes_active": 21.8 / 32, "l1_busy": 0.81}}
@@ -572,6 +576,18 @@ def main():
                     "issue": dict(NCU_ISSUE.get(dom, {}), note="ncu, one launch per kernel of an 8-render batch"),
                     "stage_ms": ps["stage_ms"], "stage_share": {k: v / max(1e-9, sum(ps["stage_ms"].values()))
                                                                 for k, v in ps["stage_ms"].items()}}
+        # The bound that applies: instruction issue.  The same kernel's warp
+        # instructions (ncu per unit x units) over its CUDA-event time,
+        # against one warp instruction per cycle per scheduler (4 per SM) at
+        # the SM clock sampled during the timed region.
+        if dom in NCU_INST_PER_UNIT:
+            mhz = clk.summary().get("sm_mhz") or 1965.0
+            sms = torch.cuda.get_device_properties(local).multi_processor_count
+            ach = NCU_INST_PER_UNIT[dom] * units / (t_ms / 1e3)
+            pk = sms * 4 * mhz * 1e6
+            roofline["issue_roofline"] = {"achieved": ach, "peak": pk, "unit": "warp instructions/s",
+                                          "frac": ach / pk, "warp_inst_per_unit": NCU_INST_PER_UNIT[dom],
+                                          "sm_mhz": mhz, "sms": sms}
 
     # ---- served stream: Poisson arrivals, continuous batching, p50/p99
     serve = None
