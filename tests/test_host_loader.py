@@ -234,3 +234,25 @@ def test_obj_normal_index_out_of_range_is_an_error(capi, tmp_path):
     with pytest.raises(capi.PcrError) as e:
         capi.HostScene(str(scene), str(tmp_path))
     assert "normal index out of range" in str(e.value)
+
+
+def test_parallel_obj_reader_reports_a_bad_index(capi, tmp_path):
+    """A face that names a vertex defined only later in the file is an error
+    for a sequential reader; the ranges-of-lines reader must report it too
+    when the face and the vertex sit in different ranges of a >1 MB file."""
+    lines = []
+    for i in range(40000):
+        lines.append("v %.6f %.6f %.6f" % (i * 1e-3, (i % 7) * 0.1, -1.0))
+    for i in range(1, 13000):
+        lines.append(f"f {3 * i - 2} {3 * i - 1} {3 * i}")
+    lines.insert(5, "f 1 2 39999")            # vertex 39999 is defined later
+    obj = tmp_path / "m.obj"
+    obj.write_text("\n".join(lines) + "\n")
+    assert obj.stat().st_size > (1 << 20)
+    scene = tmp_path / "s.json"
+    scene.write_text('{"schema": "1.0", "name": "m", "version": "1", "materials": {"w": {"albedo": [0.5,0.5,0.5]},'
+                     ' "l": {"emissive": [1,1,1]}}, "primitives": [{"type": "mesh", "file": "m.obj", "material": "w"},'
+                     ' {"type": "plane", "light": true, "origin": [0,2,0], "u": [1,0,0], "v": [0,0,1], "material": "l"}]}')
+    with pytest.raises(capi.PcrError) as e:
+        capi.HostScene(str(scene), str(tmp_path))
+    assert "vertex index out of range" in str(e.value)
