@@ -209,3 +209,33 @@ def test_wait_times_out_and_serving_restarts():
         assert np.allclose(ctx.fetch(rid)[0], ref, rtol=RTOL, atol=ATOL)
     finally:
         ctx.close()
+
+
+def test_router_mesh_scene_built_once_matches_one_context():
+    """A router scene load with triangles builds the BVH once, on the first
+    context's device, and uploads the same tree to every context: renders
+    of the mesh scene through the router equal the single-context render."""
+    from pcr_b200 import capi, workloads
+    a = capi.Context(device=0, queue_capacity=1 << 17)
+    b = capi.Context(device=0, queue_capacity=1 << 17)
+    try:
+        path = workloads.mesh_scene(59, 1)
+        router = capi.Router([a, b])
+        rsid = router.load_scene_json(path, GOLDEN)
+        sid = a.load_scene_json(path, GOLDEN)
+        reqs = [capi.render_desc(40 + 8 * k, depth=3, samples=2, shadow=2, seed=900 + k) for k in range(4)]
+        want = [a.render(sid, d)[0] for d in reqs]
+        router.serve_start()
+        tickets = [router.submit(rsid, d) for d in reqs]
+        got = []
+        for t, d in zip(tickets, reqs):
+            router.wait(t, 120_000)
+            got.append(router.fetch(t, d.width, d.height)[0])
+        router.serve_stop()
+        for w, g in zip(want, got):
+            assert np.allclose(w, g, rtol=RTOL, atol=ATOL)
+        assert min(router.load()[1]) >= 1   # both contexts rendered the mesh
+        router.close()
+    finally:
+        a.close()
+        b.close()
