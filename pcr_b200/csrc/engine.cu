@@ -1736,7 +1736,9 @@ void Engine::autotune(const int32_t* scenes, const pcr_render_desc* descs, int n
 {
     struct Cand { int q, b, c, r; };
     std::vector<Cand> cands;
-    for (int q : {1 << 19, 1 << 20, 1 << 21})
+    // up to 4M paths in flight: 16M path slots, and S = 64 shadow rays per
+    // slot still fit the 2^31-entry shadow queue
+    for (int q : {1 << 19, 1 << 20, 1 << 21, 1 << 22})
         for (int b : {64, 128, 256})
             for (int c : {1 << 14, 1 << 16})
                 for (int r : {1, 2}) cands.push_back({q, b, c, r});
