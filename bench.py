@@ -633,7 +633,7 @@ def main():
                        "parallelism": f"replicas x{world} (own seeded batch per GPU, no collective)",
                        "resolution": "square, log-uniform 128..1024", "depth": "2..8", "paths_per_pixel": "1..64",
                        "shadow_rays": "1..8", "spectral": "hero-4",
-                       "l2": "path/shadow queues ~2 GB > 126 MB L2 (no flush needed)"},
+                       "l2": "path/shadow queues (2-10 GB at the tuned 1M-4M paths in flight) > 126 MB L2 (no flush needed)"},
             "rays_per_s": rays,
             "work": {"paths": step_paths * a.steps, "rays": st["rays"], "shadow_rays": st["shadow_rays"],
                      "iterations": st.get("iterations")},
