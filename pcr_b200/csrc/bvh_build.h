@@ -13,7 +13,7 @@ namespace pcr {
 
 // verts9: n triangles as v0 v1 v2 (9 floats each).  Returns the nodes in
 // depth-first preorder and order[i] = input index of the triangle at leaf
-// position i.  Synchronous on `st`; the workspace (about 330 bytes per
+// position i.  Synchronous on `st`; the workspace (about 360 bytes per
 // triangle) comes from `pool` (null: the device's default pool).
 void device_build_bvh_raw(int device, cudaStream_t st, cudaMemPool_t pool, const float* verts9, int n,
                           std::vector<pcr_bvh_node>& nodes, std::vector<int32_t>& order);
