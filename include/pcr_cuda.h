@@ -233,9 +233,11 @@ typedef struct {
 } pcr_engine_stats;
 pcr_status pcr_engine_stats_get(pcr_ctx *ctx, pcr_engine_stats *out);
 pcr_status pcr_engine_stats_reset(pcr_ctx *ctx);
-/* Picks queue capacity, block size, chunk and refill cadence by timing short
- * trial batches of the given requests; stores the choice (and the cache file
- * when one was given). */
+/* Picks queue capacity (512K..4M paths in flight), block size, chunk and
+ * refill cadence by timing short trial batches of the given requests; stores
+ * the choice (and the cache file when one was given).  The path and shadow
+ * queues grow with the capacity: about 10 GB at 4M with up to 8 shadow rays
+ * per hit, more when requests ask for more (S slots per path slot). */
 pcr_status pcr_autotune(pcr_ctx *ctx, const pcr_scene_id *scenes, const pcr_render_desc *descs,
                         int32_t n, int32_t *chosen /* 4 ints, may be NULL */);
 
