@@ -1,18 +1,28 @@
 """Regenerates the committed test fixtures from the reference project.
 
-Run in a container that has the reference tree (default /root/reference):
+Run where the reference tree is present, naming it by argument or by the
+PCR_REFERENCE_ROOT environment variable (the reference project's top level,
+holding code/, Scenes/, models/):
 
     python tests/golden/make_fixtures.py [REFERENCE_ROOT]
 
 It copies, unmodified:
   * Scenes/*.json          -> tests/golden/scenes/   (workload definitions)
   * spd/cornell/*.spd      -> tests/golden/spd/cornell/
+  * models/*.obj           -> tests/golden/models/   (the Stanford bunny that
+                              cornell-bunny.json loads as ../models/...)
+  * luts/*.lut             -> tests/golden/luts/     (the shipped PLUT table)
   * tests/render/golden/*  -> tests/golden/render/   (the 17 golden PNGs)
+writes an emissive-mesh scene of its own (scenes/cornell-mesh-light.json
+with models/ico-light.obj: the Cornell box lit by its ceiling quad and by a
+180-triangle icosphere whose mesh primitive carries "light": true, the
+reference loader's TriangleSet light, code/Scenes/SceneLoader.cpp:449-460),
 and writes tests/golden/bvh_vectors.npz: seeded triangle soups with the
 reference's own Bvh::build node arrays and Bvh::intersect answers (via the
 compiled reference, oracle/_ref/libpcrref.so).  The GPU box has no reference
 tree, so these files are what the parity tests read there.
 """
+import json
 import os
 import shutil
 import sys
@@ -43,8 +53,33 @@ def soup_rays(seed: int, n: int) -> np.ndarray:
     return np.concatenate([o, d], 1).astype(np.float32)
 
 
+def mesh_light_scene() -> None:
+    """cornell.json plus an emissive icosphere (frequency 3, 180 triangles,
+    radius 0.3, no displacement, outward winding so every triangle's flat
+    normal faces away from its centre) hanging below the ceiling near the
+    left wall.  Two lights: the ceiling quad (a plane light) and the mesh (a
+    triangle-set light), so light picking, the cumulative-area triangle
+    pick and emissive triangles in the BVH all run."""
+    from pcr_b200 import workloads
+    tris = workloads.displaced_icosphere(3, 0, radius=0.3, amplitude=0.0)
+    os.makedirs(os.path.join(HERE, "models"), exist_ok=True)
+    workloads.write_obj(os.path.join(HERE, "models", "ico-light.obj"), tris)
+    sc = workloads.read_scene_json(os.path.join(HERE, "scenes", "cornell.json"))
+    sc["name"] = "cornell-mesh-light"
+    sc["version"] = "1.0.0"
+    sc["materials"]["coollight"] = {"emissive": [9.0, 11.0, 16.0]}
+    light = [p for p in sc["primitives"] if p.get("light")]
+    rest = [p for p in sc["primitives"] if not p.get("light")]
+    sc["primitives"] = rest + [{"type": "mesh", "file": "../models/ico-light.obj", "position": [-1.1, 1.2, -3.2],
+                                "material": "coollight", "light": True}] + light
+    with open(os.path.join(HERE, "scenes", "cornell-mesh-light.json"), "w") as f:
+        json.dump(sc, f, indent=1)
+        f.write("\n")
+
+
 def main(ref_root: str) -> None:
     for sub, pat, dst in (("Scenes", ".json", "scenes"), ("spd/cornell", ".spd", "spd/cornell"),
+                          ("models", ".obj", "models"), ("luts", ".lut", "luts"),
                           ("tests/render/golden", ".png", "render")):
         src = os.path.join(ref_root, sub)
         out = os.path.join(HERE, dst)
@@ -54,7 +89,7 @@ def main(ref_root: str) -> None:
                 shutil.copyfile(os.path.join(src, f), os.path.join(out, f))
     from oracle import ref
     if not ref.available():
-        raise SystemExit("build oracle/_ref first: make -C oracle ref")
+        raise SystemExit("build oracle/_ref first: make -C oracle ref REF=<reference>/code")
     arrays = {}
     for name, seed, n in (("soup200", 0xC0FFEE, 200), ("soup5k", 7, 5000)):
         tris = soup(seed, n)
@@ -71,8 +106,12 @@ def main(ref_root: str) -> None:
     arrays.update({"coplanar_tris": cop, "coplanar_boxes": boxes, "coplanar_ints": ints,
                    "coplanar_perm": perm})
     np.savez_compressed(os.path.join(HERE, "bvh_vectors.npz"), **arrays)
+    mesh_light_scene()
     print("fixtures written under", HERE)
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("PCR_REFERENCE_ROOT", "")
+    if not root:
+        raise SystemExit("name the reference tree: make_fixtures.py REFERENCE_ROOT (or set PCR_REFERENCE_ROOT)")
+    main(root)

@@ -10,7 +10,7 @@ import re
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, REPO, REFERENCE_ROOT, have_bunny, scene_path
+from conftest import BUNNY_SCENE, GOLDEN, REPO, have_bunny, scene_path
 
 SCENES = ["cornell", "cornell-spec", "cornell-glass", "cornell-spheres", "closed-cornell-spec",
           "cornell-large-light", "bright-cornell-glass", "closed-cornell-glass", "cornell-frank"]
@@ -64,14 +64,13 @@ def test_host_loader_matches_reference_loader(capi, name):
     assert np.array_equal(hs.planes()[:, :13].view(np.uint32), rs.planes[:, :13].view(np.uint32))
 
 
-@pytest.mark.skipif(not have_bunny(), reason="Stanford bunny OBJ only in the reference tree")
 def test_host_loader_bunny_bvh_matches_reference(capi):
     from oracle import ref
     if not ref.available():
         pytest.skip("reference harness not built")
-    path = os.path.join(REFERENCE_ROOT, "Scenes", "cornell-bunny.json")
-    hs = capi.HostScene(path, REFERENCE_ROOT)
-    rs = ref.load_scene(path, REFERENCE_ROOT)
+    assert have_bunny(), "the Stanford bunny fixture (tests/golden/models) is missing"
+    hs = capi.HostScene(BUNNY_SCENE, GOLDEN)
+    rs = ref.load_scene(BUNNY_SCENE, GOLDEN)
     assert np.array_equal(hs.triangles()[:, :21].view(np.uint32), rs.triangles[:, :21].view(np.uint32))
     b = hs.bvh()
     assert np.array_equal(b[:, :6].view(np.uint32), rs.bvh_boxes.view(np.uint32))

@@ -8,7 +8,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import GOLDEN, REFERENCE_ROOT, have_bunny, scene_path
+from conftest import BUNNY_SCENE, GOLDEN, have_bunny, scene_path
 
 # (golden name, scene, renderer knobs) from the reference's render suite
 GOLDENS = [
@@ -57,19 +57,17 @@ def test_oracle_lut_goldens(oracle_lib, built_lut, name):
 
 
 def test_oracle_lut_matches_shipped_plut(built_lut):
-    path = os.path.join(REFERENCE_ROOT, "luts", "default-kres16.lut")
-    if not os.path.exists(path):
-        pytest.skip("reference LUT file not present")
+    path = os.path.join(GOLDEN, "luts", "default-kres16.lut")
     raw = open(path, "rb").read()
     assert raw[:4] == b"PLUT"
     assert np.array_equal(np.frombuffer(raw[16:], np.float32).view(np.uint32), built_lut.view(np.uint32))
 
 
-@pytest.mark.skipif(not have_bunny(), reason="Stanford bunny OBJ only in the reference tree")
 @pytest.mark.parametrize("name,kw", [("cornell-bunny-rgb", {}), ("cornell-bunny-spectral", {"spectral": True})])
 def test_oracle_bunny_goldens(oracle_lib, name, kw):
     O = oracle_lib
-    sc = O.load_scene(os.path.join(REFERENCE_ROOT, "Scenes", "cornell-bunny.json"), REFERENCE_ROOT)
+    assert have_bunny(), "the Stanford bunny fixture (tests/golden/models) is missing"
+    sc = O.load_scene(BUNNY_SCENE, GOLDEN)
     _, rgb = O.render(sc, O.opts(120, **kw))
     assert np.array_equal(rgb, _golden(name))
 
