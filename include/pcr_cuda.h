@@ -3,7 +3,7 @@
  * This is the drop-in boundary for pcr's GPU backend.  In the reference the
  * GPU renderer is chosen by a compile-time alias (code/Gpu/GpuRenderer.h:15-21)
  * and driven through the OpenglRenderer/MetalRenderer surface
- * (code/Gpu/Opengl/OpenglRenderer.h:50-138): a constructor taking
+ * (code/Gpu/Opengl/OpenglRenderer.h:29-117): a constructor taking
  * (width, height, depth, samples, shadowSamples), public quality knobs, and
  * render(const Scenes::SceneData&, start, outputDir).  A CudaRenderer class
  * with that surface (pcr_b200/csrc/cuda_renderer.h) wraps the calls below.
@@ -218,10 +218,22 @@ pcr_status pcr_wait(pcr_ctx *ctx, pcr_request_id id, int64_t timeout_ms);
 /* Copies the finished result out and frees the request's device memory. */
 pcr_status pcr_fetch(pcr_ctx *ctx, pcr_request_id id, float *hdr_out, uint8_t *rgb8_out,
                      pcr_render_stats *stats);
-/* Cancels a request still waiting for admission (PCR_ERR_INVALID once it
- * runs).  pcr_wait on it then returns PCR_ERR_CANCELLED; pcr_fetch returns
- * PCR_ERR_CANCELLED and releases it. */
+/* Cancels a request, the counterpart of the reference renderers'
+ * cancelRequested flag (code/Renderer.cpp:170-181,
+ * code/Gpu/Opengl/OpenglRenderer.cpp:2170-2175).  A request waiting for
+ * admission is dropped at once; a running one stops issuing paths at the
+ * next block of iterations and ends when the paths in flight retire (within
+ * its depth in iterations), its partial result discarded; a finished one
+ * keeps its result (the call is then a no-op).  pcr_wait on a cancelled
+ * request returns PCR_ERR_CANCELLED; pcr_fetch returns PCR_ERR_CANCELLED
+ * and releases it. */
 pcr_status pcr_cancel(pcr_ctx *ctx, pcr_request_id id);
+/* Share of a request's paths traced to the end, in [0, 1], from the device
+ * state copied after each block of iterations: 0 while it waits for
+ * admission, 1 once it is resolved.  The counterpart of the reference's
+ * progressRows counter (code/Includes/Renderer.h:41-43), which the
+ * CudaRenderer surface fills as fraction x height. */
+pcr_status pcr_progress(pcr_ctx *ctx, pcr_request_id id, double *fraction);
 
 /* ------------------------------------------------------------- engine info */
 typedef struct {
@@ -248,7 +260,7 @@ pcr_status pcr_autotune(pcr_ctx *ctx, const pcr_scene_id *scenes, const pcr_rend
  * 3 triangle id from triangle_ids) and t.  Host buffers. */
 pcr_status pcr_trace_closest(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, int64_t n,
                              int32_t *mat, int32_t *prim, float *t);
-/* Bvh::intersect over the triangles only (code/Bvh/Bvh.cpp:419-510), with
+/* Bvh::intersect over the triangles only (code/Bvh/Bvh.cpp:353-444), with
  * per-ray counts of internal nodes visited and triangles tested (may be NULL). */
 pcr_status pcr_trace_bvh(pcr_ctx *ctx, pcr_scene_id scene, const float *rays, int64_t n,
                          int32_t *tri_id, float *t, int32_t *counts);
@@ -299,7 +311,10 @@ pcr_status pcr_bvh_build(pcr_ctx *ctx, const pcr_triangle *tris, int32_t n, pcr_
 /* Device evaluations of the FP32 stage functions on a wavelength / colour grid:
  * what 0 sigmoid fit at lambda (fit=4 floats) | 1 tabulated spectrum (61) |
  * 2 CIE xbar/ybar/zbar (3 out) | 3 singleLambdaXYZ(lambda, in[i]) (3 out) |
- * 4 XYZ->linear sRGB (3 in/out) | 5 Reinhard (3) | 6 ACES (3) | 7 8-bit quantise (3). */
+ * 4 XYZ->linear sRGB (3 in/out) | 5 Reinhard (3) | 6 ACES (3) | 7 8-bit quantise (3) |
+ * 8 singleLambdaXYZ(lambda, in[i]) as the hot path forms it (3 out): the
+ * interpolated colour-matching table that raygen reads, times the radiance
+ * (code/Includes/CIE.h:140-159). */
 pcr_status pcr_eval_stage(pcr_ctx *ctx, int32_t what, const float *params, const float *in,
                           int64_t n, float *out);
 

@@ -25,7 +25,7 @@ EXPORTS = [
     "pcr_scene_upload", "pcr_scene_load_json", "pcr_host_scene_load", "pcr_host_scene_free",
     "pcr_fit_sigmoid", "pcr_lut_build", "pcr_scene_release", "pcr_scene_bytes", "pcr_render", "pcr_render_noalloc",
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
-    "pcr_fetch", "pcr_cancel", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
+    "pcr_fetch", "pcr_cancel", "pcr_progress", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
     "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_bvh_build", "pcr_eval_stage",
     "pcr_tonemap", "pcr_router_create", "pcr_router_destroy", "pcr_router_scene_load_json", "pcr_router_serve_start",
     "pcr_router_serve_stop", "pcr_router_submit", "pcr_router_wait", "pcr_router_fetch", "pcr_router_load",
@@ -152,6 +152,7 @@ def load_library():
         "pcr_wait": [P, C.c_int64, C.c_int64],
         "pcr_fetch": [P, C.c_int64, fp, up, C.POINTER(RenderStats)],
         "pcr_cancel": [P, C.c_int64],
+        "pcr_progress": [P, C.c_int64, C.POINTER(C.c_double)],
         "pcr_engine_stats_get": [P, C.POINTER(EngineStats)],
         "pcr_engine_stats_reset": [P],
         "pcr_autotune": [P, ip, C.POINTER(RenderDesc), C.c_int32, ip],
@@ -272,6 +273,7 @@ class Context:
                  chunk_paths: int = 0, regen_every: int = 0, use_graph: bool = True, profile: bool = False,
                  tuning_cache: str | None = None):
         self.L = load_library()
+        self.device = device
         self._cache = tuning_cache.encode() if tuning_cache else None
         o = CtxOpts(device, memory_budget, queue_capacity, block_size, chunk_paths, regen_every, int(use_graph),
                     int(profile), self._cache)
@@ -390,6 +392,11 @@ class Context:
     def cancel(self, rid: int) -> None:
         _check(self.L.pcr_cancel(self.h, rid))
 
+    def progress(self, rid: int) -> float:
+        f = C.c_double()
+        _check(self.L.pcr_progress(self.h, rid, C.byref(f)))
+        return f.value
+
     def stats(self) -> dict:
         s = EngineStats()
         _check(self.L.pcr_engine_stats_get(self.h, C.byref(s)))
@@ -463,7 +470,7 @@ class Context:
 
     def eval_stage(self, what: int, inp: np.ndarray, params: np.ndarray | None = None) -> np.ndarray:
         x = np.ascontiguousarray(inp, np.float32)
-        widths_in = {0: 1, 1: 1, 2: 1, 3: 2, 4: 3, 5: 3, 6: 3, 7: 3}
+        widths_in = {0: 1, 1: 1, 2: 1, 3: 2, 4: 3, 5: 3, 6: 3, 7: 3, 8: 2}
         n = x.size // widths_in[what]
         out = np.zeros((n, 1 if what in (0, 1) else 3), np.float32)
         p = np.ascontiguousarray(params, np.float32) if params is not None else None

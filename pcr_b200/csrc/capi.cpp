@@ -276,6 +276,14 @@ pcr_status pcr_cancel(pcr_ctx* ctx, pcr_request_id id)
     return guard([&] { E(ctx).cancel(id); });
 }
 
+pcr_status pcr_progress(pcr_ctx* ctx, pcr_request_id id, double* fraction)
+{
+    return guard([&] {
+        if (!fraction) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *fraction = E(ctx).progress(id);
+    });
+}
+
 pcr_status pcr_engine_stats_get(pcr_ctx* ctx, pcr_engine_stats* out)
 {
     return guard([&] {

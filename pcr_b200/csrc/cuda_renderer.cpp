@@ -156,7 +156,38 @@ bool CudaRenderer::render_to(const pcr_scene_desc& scene, RenderOutput& out)
     out.hdr.assign((size_t)_width * _height * 3, 0.f);
     out.rgb8.assign((size_t)_width * _height * 3, 0);
     pcr_render_stats st{};
-    if (pcr_render(_ctx, _scene, &d, out.hdr.data(), out.rgb8.data(), &st) != PCR_OK) {
+    pcr_request_id id = -1;
+    if (pcr_submit(_ctx, _scene, &d, &id) != PCR_OK) {
+        std::cerr << "pcr: render failed: " << pcr_last_error() << std::endl;
+        return false;
+    }
+    // The render runs as blocks of graph-captured iterations driven from this
+    // thread.  Between blocks the loop reports progress and honours a cancel
+    // request, as the reference renderers poll between pixels or tiles
+    // (code/Renderer.cpp:170-181, code/Gpu/Opengl/OpenglRenderer.cpp:2170-2175).
+    bool cancel_sent = false;
+    while (true) {
+        const pcr_status w = pcr_wait(_ctx, id, 20);
+        if (w == PCR_OK) break;
+        if (w == PCR_ERR_CANCELLED) {
+            pcr_fetch(_ctx, id, nullptr, nullptr, nullptr);  // reports the cancel and releases the request
+            if (progressRows) progressRows->store(0, std::memory_order_relaxed);
+            std::cout << "GPU render cancelled." << std::endl;
+            return false;
+        }
+        if (w != PCR_ERR_TIMEOUT) {
+            std::cerr << "pcr: render failed: " << pcr_last_error() << std::endl;
+            return false;
+        }
+        double f = 0.0;
+        if (progressRows && pcr_progress(_ctx, id, &f) == PCR_OK)
+            progressRows->store((int)(f * _height), std::memory_order_relaxed);
+        if (!cancel_sent && cancelRequested && cancelRequested->load(std::memory_order_relaxed)) {
+            pcr_cancel(_ctx, id);
+            cancel_sent = true;
+        }
+    }
+    if (pcr_fetch(_ctx, id, out.hdr.data(), out.rgb8.data(), &st) != PCR_OK) {
         std::cerr << "pcr: render failed: " << pcr_last_error() << std::endl;
         return false;
     }

@@ -1,7 +1,7 @@
 // CudaRenderer: the reference GPU renderer's public surface on top of the C
 // ABI (include/pcr_cuda.h).
 //
-// Mirrors code/Gpu/Opengl/OpenglRenderer.h:50-138 and the CPU Renderer's
+// Mirrors code/Gpu/Opengl/OpenglRenderer.h:29-117 and the CPU Renderer's
 // knobs (code/Includes/Renderer.h:41-109): the (width, height, depth,
 // samples, shadowSamples, sharedContext) constructor, the public quality
 // fields, render(scene, start, outputDir) writing the tone-mapped PNG with

@@ -51,6 +51,18 @@ __global__ void k_set_active(EngineView E, ActiveList L)
 
 __global__ void k_set_params(EngineParams* P, EngineParams p) { *P = p; }
 
+// Cancels a running request: no path of it is issued after this point
+// (its total becomes what was issued so far), so it finishes once the paths
+// already in flight retire, within `depth` iterations.  Launched between
+// blocks of iterations on the engine stream, so no kernel reads the entry
+// while it changes.
+__global__ void k_cancel(EngineView E, int slot)
+{
+    DRequest& R = const_cast<DRequest&>(E.reqs[slot]);
+    R.flags |= kReqCancelled;
+    R.total = (long long)E.issued[slot];
+}
+
 // ---------------------------------------------------------------- helpers
 static float host_ybar_integral()
 {
@@ -869,6 +881,20 @@ void Engine::launch_iteration(int cur, bool prof)
     iterations_++;
 }
 
+// k_shade's limit on dynamic shared memory is one attribute of the function
+// on the current device, shared by every context of the process.  It is only
+// ever raised: a context with a smaller material table must not lower it
+// below the size another context's launches (or captured graph) use.
+static void raise_shade_smem(size_t bytes)
+{
+    static std::mutex mu;
+    std::lock_guard<std::mutex> g(mu);
+    cudaFuncAttributes a{};
+    CK(cudaFuncGetAttributes(&a, (const void*)k_shade));
+    if ((int)bytes > a.maxDynamicSharedSizeBytes)
+        CK(cudaFuncSetAttribute((const void*)k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+}
+
 void Engine::build_graph()
 {
     const int B = tune_.block_size;
@@ -876,7 +902,7 @@ void Engine::build_graph()
     const size_t mat_bytes = sizeof(DMaterial) * (size_t)std::max(1, mat_count_);
     smem_mats_ = mat_bytes <= 96 * 1024 ? 1 : 0;
     shade_smem_ = smem_mats_ ? mat_bytes : 0;
-    CK(cudaFuncSetAttribute(k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)std::max<size_t>(shade_smem_, 0)));
+    raise_shade_smem(shade_smem_);
     grid_for((const void*)k_regen, B, 0, &grid_regen_);
     grid_for((const void*)k_extend, B, 0, &grid_extend_);
     grid_for((const void*)k_shade, kShadeBlock, shade_smem_, &grid_shade_);
@@ -947,6 +973,19 @@ void Engine::finish_request(Request& r)
     r.state = ReqState::Resolving;
 }
 
+// A cancelled request whose in-flight paths have retired: its device
+// memory goes back to the pool (stream-ordered after the iterations that
+// wrote it) and it waits in the Cancelled state for the fetch that reports
+// and releases it.
+void Engine::release_cancelled(Request& r)
+{
+    for (void** p : {(void**)&r.accum, (void**)&r.d_hdr, (void**)&r.d_rgb, (void**)&r.act[0], (void**)&r.act[1],
+                     (void**)&r.welford})
+        if (*p) { CK(cudaFreeAsync(*p, stream_)); *p = nullptr; }
+    r.state = ReqState::Cancelled;
+    r.t_ready = std::chrono::steady_clock::now();
+}
+
 // Copies a resolved request's images to caller host buffers through one
 // reusable pinned staging buffer on the copy stream (ordered after the
 // resolve by the request's event), then frees its device images.
@@ -988,7 +1027,8 @@ void Engine::harvest(bool)
             const unsigned long long tf = h_snap_->tf[s], td = h_snap_->td[s];
             r.device_ms = (td > tf && tf) ? (double)(td - tf) * 1e-6 : 0.0;
             r.paths = h_snap_->issued[s];  // adaptive requests trace fewer than W*H*spp*aa
-            finish_request(r);
+            if (r.cancel_running) release_cancelled(r);
+            else finish_request(r);
             slot_owner_[s] = -1;
             bytes_in_use_ -= r.bytes;
             active_dirty_ = true;
@@ -1023,6 +1063,14 @@ bool Engine::engine_step()
         std::lock_guard<std::mutex> g(mu_);
         admit_locked();
         upload_active();
+        for (int s : active_slots_) {
+            Request& r = *reqs_[slot_owner_[s]];
+            if (r.cancel_running && !r.cancel_sent) {
+                k_cancel<<<1, 1, 0, stream_>>>(view(), s);
+                CK(cudaGetLastError());
+                r.cancel_sent = true;
+            }
+        }
         bool resolving = false;
         for (auto& kv : reqs_)
             if (kv.second->state == ReqState::Resolving) { resolving = true; break; }
@@ -1050,6 +1098,7 @@ bool Engine::engine_step()
     CK(cudaMemcpyAsync(hs->tf, d_tfirst_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(hs->td, d_tdone_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
     CK(cudaMemcpyAsync(hs->issued, d_issued_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaMemcpyAsync(hs->outstanding, d_outstanding_, 8 * kMaxActive, cudaMemcpyDeviceToHost, stream_));
     CK(cudaEventRecord(ev_snaps_[b], stream_));
     snap_next_ = (snap_next_ + 1) % kSnapRing;
     snap_inflight_++;
@@ -1219,14 +1268,40 @@ void Engine::fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st)
 
 void Engine::cancel(int64_t id)
 {
+    {
+        std::lock_guard<std::mutex> g(mu_);
+        auto it = reqs_.find(id);
+        if (it == reqs_.end()) throw PcrError(PCR_ERR_NOT_FOUND, "unknown request");
+        Request& r = *it->second;
+        if (r.state == ReqState::Pending) {
+            r.state = ReqState::Cancelled;
+            return;
+        }
+        // a running request stops issuing paths at the next block of
+        // iterations (engine_step sends it to the device); a finished one
+        // keeps its result
+        if (r.state != ReqState::Active) return;
+        r.cancel_running = true;
+    }
+    cv_.notify_all();
+}
+
+// Share of a request's paths that have been traced to the end (issued and
+// retired), from the device state copied after the last harvested block:
+// 0 while it waits for admission, 1 once its images are resolved.
+double Engine::progress(int64_t id)
+{
     std::lock_guard<std::mutex> g(mu_);
     auto it = reqs_.find(id);
     if (it == reqs_.end()) throw PcrError(PCR_ERR_NOT_FOUND, "unknown request");
-    if (it->second->state == ReqState::Pending) {
-        it->second->state = ReqState::Cancelled;
-        return;
-    }
-    throw PcrError(PCR_ERR_INVALID, "only pending requests can be cancelled");
+    const Request& r = *it->second;
+    if (r.state == ReqState::Pending) return 0.0;
+    if (r.state != ReqState::Active) return 1.0;
+    if (!h_snap_ || h_snap_block_ <= r.admit_block) return 0.0;
+    const pcr_render_desc& d = r.desc;
+    const double total = (double)d.width * d.height * local_spp(d) * std::max(1, d.aa_samples);
+    const double retired = (double)h_snap_->issued[r.slot] - (double)h_snap_->outstanding[r.slot];
+    return std::min(1.0, std::max(0.0, retired / std::max(1.0, total)));
 }
 
 // ---------------------------------------------------------------- plain method
@@ -1505,7 +1580,7 @@ void Engine::render_noalloc(int scene, const pcr_render_desc& desc, float* hdr_d
     const size_t mat_bytes = sizeof(DMaterial) * (size_t)std::max(1, mat_count_);
     const int smem_mats = mat_bytes <= 96 * 1024 ? 1 : 0;
     const size_t smem = smem_mats ? mat_bytes : 0;
-    CK(cudaFuncSetAttribute(k_shade, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raise_shade_smem(smem);
     int g_regen, g_extend, g_shade, g_shadow;
     grid_for((const void*)k_regen, B, 0, &g_regen);
     grid_for((const void*)k_extend, B, 0, &g_extend);
@@ -1668,8 +1743,8 @@ void Engine::eval_stage(int what, const float* params, const float* in, int64_t 
 {
     std::lock_guard<std::mutex> g(run_mu_);
     CK(cudaSetDevice(device_));
-    if (what < 0 || what > 7 || n <= 0) throw PcrError(PCR_ERR_INVALID, "bad stage evaluation request");
-    const int in_w = (what == 0 || what == 1 || what == 2) ? 1 : (what == 3 ? 2 : 3);
+    if (what < 0 || what > 8 || n <= 0) throw PcrError(PCR_ERR_INVALID, "bad stage evaluation request");
+    const int in_w = (what == 0 || what == 1 || what == 2) ? 1 : ((what == 3 || what == 8) ? 2 : 3);
     const int out_w = (what == 0 || what == 1) ? 1 : 3;
     const int np = what == 0 ? 4 : (what == 1 ? kSpecN : 0);
     float *d_in = nullptr, *d_out = nullptr, *d_p = nullptr;
@@ -1681,7 +1756,8 @@ void Engine::eval_stage(int what, const float* params, const float* in, int64_t 
         if (!params) throw PcrError(PCR_ERR_INVALID, "stage needs parameters");
         CK(cudaMemcpyAsync(d_p, params, np * sizeof(float), cudaMemcpyHostToDevice, stream_));
     }
-    k_eval_stage<<<std::min<int64_t>((n + 255) / 256, 4096), 256, 0, stream_>>>(what, d_p, d_in, n, d_out, xyz_scale_);
+    k_eval_stage<<<std::min<int64_t>((n + 255) / 256, 4096), 256, 0, stream_>>>(what, d_p, d_in, n, d_out, xyz_scale_,
+                                                                                 d_cmf_);
     CK(cudaGetLastError());
     CK(cudaMemcpyAsync(out, d_out, n * out_w * sizeof(float), cudaMemcpyDeviceToHost, stream_));
     CK(cudaFreeAsync(d_in, stream_));

@@ -53,6 +53,8 @@ struct Request {
     double device_ms = 0;
     uint64_t paths = 0;
     uint64_t admit_block = 0;  // blocks launched before this request's slot was (re)set
+    bool cancel_running = false;        // cancel asked while Active
+    bool cancel_sent = false;           // k_cancel launched for it
     int* act[2] = {nullptr, nullptr};   // adaptive: pixel lists of alternate rounds
     float4* welford = nullptr;          // adaptive: per-pixel mean / M2
 };
@@ -86,6 +88,7 @@ public:
     void wait(int64_t id, int64_t timeout_ms);
     void fetch(int64_t id, float* hdr, uint8_t* rgb, pcr_render_stats* st);
     void cancel(int64_t id);
+    double progress(int64_t id);
 
     void trace(int scene, const float* rays, int64_t n, int32_t* mat, int32_t* prim, float* t, int bvh_only,
                int32_t* counts);
@@ -117,6 +120,7 @@ private:
     void build_graph();
     void harvest(bool final_sync);
     void finish_request(Request& r);
+    void release_cancelled(Request& r);
     void copy_out(Request& r, float* hdr, uint8_t* rgb);
     DRequest make_request(const pcr_render_desc& d, int scene, double* accum) const;
     void check_status();
@@ -159,6 +163,7 @@ private:
         Counters cnt;
         int done[kMaxActive];
         unsigned long long tf[kMaxActive], td[kMaxActive], issued[kMaxActive];
+        long long outstanding[kMaxActive];
     };
     // Device state copied out after each block of iterations, into a ring of
     // pinned buffers: the host keeps up to kSnapRing blocks queued and

@@ -55,7 +55,8 @@ __global__ void __launch_bounds__(kSchedThreads) k_schedule(EngineView E, const 
             // an adaptive round ended last iteration and k_round kept
             // round_cnt pixels: open the next round, or finish the request
             DRequest& R = const_cast<DRequest&>(E.reqs[slot]);
-            const int kept = E.round_cnt[slot];
+            // a cancelled request opens no further round
+            const int kept = (R.flags & kReqCancelled) ? 0 : E.round_cnt[slot];
             E.round_cnt[slot] = 0;
             E.round_state[slot] = 0;
             R.round_base = R.total;
@@ -125,27 +126,46 @@ struct XyzWeights {
     float3 w[4];
 };
 
-// The colour-matching functions tabulated at kCmfStep nm over [400, 700]
-// from the exact device cmf() (seven correctly rounded exponentials per
-// wavelength), read back with linear interpolation.  The interpolation
-// error is below 1e-7 of each function's peak and below 5e-6 relative
-// (the worst case is x-bar near 500 nm, where its lobes cancel), and raygen
-// evaluates four wavelengths per path without 28 double-precision
-// exponentials.
-constexpr float kCmfStep = 0.0125f;
-constexpr int kCmfEntries = 24001;  // (700 - 400) / kCmfStep + 1
+// The colour-matching functions tabulated every 1/kCmfPerNm nm over
+// [kCmfLo, kCmfHi] (380..720 nm, wider than the 400..700 nm the hero
+// wavelengths span) and read back with linear interpolation, so raygen
+// evaluates four wavelengths per path without 28 exponentials.  Entries are
+// the Wyman-Sloan-Shirley lobes (code/Includes/CIE.h:27-53, their float
+// constants) evaluated in double at the exact grid wavelength, then rounded
+// once; the lookup's fraction comes from one fused multiply-add of the exact
+// difference lambda - kCmfLo, so the only error left is the interpolation's.
+// Against the reference's float evaluation (singleLambdaXYZ) the result
+// stays below 1e-5 relative, or 1e-7 absolute near zero, over 380..720 nm
+// (x-bar near 508 nm, where its lobes cancel, is the tightest point).
+constexpr float kCmfLo = 380.f, kCmfHi = 720.f;
+constexpr int kCmfPerNm = 80;
+constexpr int kCmfEntries = 340 * kCmfPerNm + 1;  // (kCmfHi - kCmfLo) * kCmfPerNm + 1
+__device__ __forceinline__ double wyman_d(double l, float mu, float s1, float s2)
+{
+    const double t = (l < (double)mu) ? (l - (double)mu) * (double)s1 : (l - (double)mu) * (double)s2;
+    return exp(-0.5 * t * t);
+}
 __global__ void k_cmf_table(float4* table)
 {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < kCmfEntries; i += gridDim.x * blockDim.x) {
-        const float3 c = cmf(400.f + (float)i * kCmfStep);
-        table[i] = make_float4(c.x, c.y, c.z, 0.f);
+        const double l = (double)kCmfLo + (double)i / (double)kCmfPerNm;
+        const double x = (double)0.362f * wyman_d(l, 442.0f, 0.0624f, 0.0374f) +
+                         (double)1.056f * wyman_d(l, 599.8f, 0.0264f, 0.0323f) -
+                         (double)0.065f * wyman_d(l, 501.1f, 0.0490f, 0.0382f);
+        const double y = (double)0.821f * wyman_d(l, 568.8f, 0.0213f, 0.0247f) +
+                         (double)0.286f * wyman_d(l, 530.9f, 0.0613f, 0.0322f);
+        const double z = (double)1.217f * wyman_d(l, 437.0f, 0.0845f, 0.0278f) +
+                         (double)0.681f * wyman_d(l, 459.0f, 0.0385f, 0.0725f);
+        table[i] = make_float4((float)x, (float)y, (float)z, 0.f);
     }
 }
 __device__ __forceinline__ float3 cmf_lut(const float4* __restrict__ table, float l)
 {
-    const float t = fminf(fmaxf((l - 400.f) * (1.f / kCmfStep), 0.f), (float)(kCmfEntries - 1));
-    const int i = min((int)t, kCmfEntries - 2);
-    const float f = t - (float)i;
+    // l - kCmfLo is exact for l in [190, 760] (Sterbenz); fmaf rounds
+    // d * kCmfPerNm - i once, so f carries no error from the product
+    const float d = l - kCmfLo;
+    const int i = min(max((int)floorf(d * (float)kCmfPerNm), 0), kCmfEntries - 2);
+    const float f = fmaf(d, (float)kCmfPerNm, -(float)i);
     const float4 a = table[i], b = table[i + 1];
     return make_float3(a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f, a.z + (b.z - a.z) * f);
 }
@@ -861,7 +881,8 @@ __global__ void k_status(EngineView E, int next)
         if (E.round_state[slot]) { s_busy = 1; continue; }
         const bool all_issued = (long long)E.issued[slot] >= E.reqs[slot].total;
         if (all_issued && E.outstanding[slot] == 0) {
-            if (E.reqs[slot].flags & kReqAdaptive) {
+            // a cancelled adaptive request opens no further round
+            if ((E.reqs[slot].flags & (kReqAdaptive | kReqCancelled)) == kReqAdaptive) {
                 E.round_state[slot] = 1;  // k_round, then the next k_schedule
                 E.round_list[atomicAdd(&C->n_rounds, 1)] = slot;
                 s_busy = 1;
@@ -1062,7 +1083,7 @@ __global__ void k_trace_shadow(const DScene* scene, const DMaterial* mats, const
 }
 
 __global__ void k_eval_stage(int what, const float* __restrict__ params, const float* __restrict__ in, long long n,
-                             float* __restrict__ out, float xyz_scale)
+                             float* __restrict__ out, float xyz_scale, const float4* __restrict__ cmf_table)
 {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         switch (what) {
@@ -1079,6 +1100,14 @@ __global__ void k_eval_stage(int what, const float* __restrict__ params, const f
         case 5: for (int k = 0; k < 3; k++) out[i * 3 + k] = reinhard(in[i * 3 + k]); break;
         case 6: for (int k = 0; k < 3; k++) out[i * 3 + k] = aces(in[i * 3 + k]); break;
         case 7: for (int k = 0; k < 3; k++) out[i * 3 + k] = (float)quantize(in[i * 3 + k]); break;
+        case 8: {
+            // the XYZ weight raygen stores for a one-wavelength path (the
+            // colour-matching table), times the radiance: singleLambdaXYZ
+            const float lam[4] = {in[i * 2], in[i * 2], in[i * 2], in[i * 2]};
+            const XyzWeights W = xyz_weights(true, lam, 1, 1.f, xyz_scale, cmf_table);
+            const float r = in[i * 2 + 1];
+            out[i * 3] = r * W.w[0].x; out[i * 3 + 1] = r * W.w[0].y; out[i * 3 + 2] = r * W.w[0].z;
+        } break;
         default: break;
         }
     }

@@ -111,7 +111,7 @@ struct DScene {
 
 // Request flags
 constexpr int kReqSpectral = 1, kReqMIS = 2, kReqRussian = 4, kReqStratified = 8, kReqAdaptive = 16,
-              kReqTerminate = 32;
+              kReqTerminate = 32, kReqCancelled = 64;
 
 struct DRequest {
     int scene, width, height, depth;

@@ -93,3 +93,33 @@ def test_cli_spectral_terminate_matches_library(tmp_path, terminate):
     ctx.close()
     assert np.array_equal(rgb, lib[int(terminate)])
     assert not np.array_equal(lib[0], lib[1])
+
+
+def test_renderer_progress_and_cancel(tmp_path):
+    """pcr::CudaRenderer polls cancelRequested and fills progressRows between
+    blocks of iterations, as the reference renderers poll between pixels or
+    tiles (code/Renderer.cpp:170-181, code/Gpu/Opengl/OpenglRenderer.cpp:
+    2170-2175).  A 1024x1024 render of 1024 paths per pixel, cancelled from
+    another thread once its progress moves, returns within a fraction of a
+    second of the cancel and writes no PNG; the next render completes with
+    progressRows = height."""
+    from pcr_b200 import build
+    build.build()
+    exe = str(tmp_path / "renderer_cancel")
+    lib = os.path.join(REPO, "pcr_b200", "lib")
+    cmd = ["g++", "-std=c++17", "-O2", "-o", exe, os.path.join(REPO, "tests", "cpp", "renderer_cancel.cpp"),
+           os.path.join(REPO, "pcr_b200", "csrc", "cuda_renderer.cpp"), "-I", os.path.join(REPO, "include"),
+           "-I", os.path.join(REPO, "pcr_b200", "csrc"), "-I", "/usr/local/cuda/include", "-L", lib, "-lpcr_b200",
+           "-Wl,-rpath," + lib, "-lz", "-lpthread"]
+    out = subprocess.run(cmd, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    out = subprocess.run([exe, scene_path("cornell"), GOLDEN, str(tmp_path / "png")], capture_output=True, text=True,
+                         timeout=300)
+    assert out.returncode == 0, out.stderr[-3000:]
+    line = [x for x in out.stdout.splitlines() if x.startswith("rows_at_cancel=")][-1]
+    r = dict(kv.split("=") for kv in line.split())
+    assert int(r["rows_at_cancel"]) > 0, line          # progress moved while it ran
+    assert r["big_written"] == "0", line               # cancelled: no PNG
+    assert float(r["cancel_to_return"]) < 1.0, line    # the paths in flight retire, no more are issued
+    assert "GPU render cancelled." in out.stdout
+    assert r["small_written"] == "1" and int(r["small_rows"]) == 48, line

@@ -117,6 +117,44 @@ def test_shadow_test_matches_oracle(ctx, O, name):
     ctx.release_scene(sid)
 
 
+def test_shadow_test_matches_oracle_with_mesh_light(ctx, O):
+    """The emissive-mesh scene (a 180-triangle icosphere whose mesh primitive
+    is a light, beside the ceiling quad): emissive triangles sit in the BVH,
+    so the shadow query takes the closest-hit route, where a hit on an
+    emissive triangle never blocks.  A third of the segments end on the
+    light triangles, a third on the quad, the rest anywhere in the box."""
+    name = "cornell-mesh-light"
+    sid = ctx.load_scene_json(scene_path(name), GOLDEN)
+    osc = O.load_scene(scene_path(name), GOLDEN)
+    tl = [t for kind, payload in osc.lights if kind == 1 for t in payload]
+    assert len(tl) == 180
+    n = 150_000
+    rays, d2 = _shadow_rays(osc, n, 91)
+    rng = np.random.default_rng(92)
+    o = box_rays(n // 3, 93)[:, :3]
+    k = rng.integers(0, len(tl), n // 3)
+    a, b = rng.uniform(size=n // 3), rng.uniform(size=n // 3)
+    flip = a + b > 1
+    a[flip], b[flip] = 1 - a[flip], 1 - b[flip]
+    v = np.array([[list(t.v0), list(t.v1), list(t.v2)] for t in tl], np.float32)[k]
+    P = (v[:, 0] + (v[:, 1] - v[:, 0]) * a[:, None] + (v[:, 2] - v[:, 0]) * b[:, None]).astype(np.float32)
+    Li = (P - o).astype(np.float32)
+    dd = (Li[:, 0] * Li[:, 0] + Li[:, 1] * Li[:, 1] + Li[:, 2] * Li[:, 2]).astype(np.float32)
+    ok = dd > 1e-6
+    mr = np.concatenate([o[ok], Li[ok] / np.sqrt(dd[ok])[:, None]], 1).astype(np.float32)
+    rays, d2 = np.concatenate([rays, mr]), np.concatenate([d2, dd[ok]])
+    got = ctx.trace_shadow(sid, rays, d2).astype(bool)
+    want, marginal = _oracle_blocked(O, osc, rays, d2)
+    bad = (got != want) & ~marginal
+    assert bad.sum() == 0, f"{bad.sum()} shadow decisions differ ({(got != want).sum()} incl. marginal)"
+    # segments that end on the light mesh: some blocked (origins inside or
+    # behind the boxes), most lit (a hit on the mesh's emissive near side
+    # never blocks, code/Renderer.cpp:860)
+    tail = want[-mr.shape[0]:]
+    assert 0.05 < tail.mean() < 0.95
+    ctx.release_scene(sid)
+
+
 def _oracle_bvh_query(O, nodes, arr, rays, chunks=64):
     parts = np.array_split(np.arange(rays.shape[0]), chunks)
     with ThreadPoolExecutor(max_workers=os.cpu_count() or 4) as ex:
@@ -256,6 +294,13 @@ def test_stage_functions_match_oracle(ctx, O):
     g = ctx.eval_stage(3, np.stack([lam, rad], 1))
     L.oracle_single_lambda_xyz(fptr(lam), fptr(rad), lam.size, fptr(c))
     assert _rel_ok(g, c)
+    # the form the hot path uses: raygen's interpolated colour-matching table
+    # (the weight a path carries) times the radiance, 380..720 nm
+    g = ctx.eval_stage(8, np.stack([lam, rad], 1))
+    assert _rel_ok(g, c), "table-interpolated singleLambdaXYZ beyond 1e-5 relative"
+    one = np.ones_like(lam)
+    L.oracle_single_lambda_xyz(fptr(lam), fptr(one), lam.size, fptr(c))
+    assert _rel_ok(ctx.eval_stage(8, np.stack([lam, one], 1)), c)
     # XYZ -> sRGB, Reinhard, ACES, quantisation
     xyz = np.random.default_rng(2).uniform(-0.2, 4.0, (100000, 3)).astype(np.float32)
     g = ctx.eval_stage(4, xyz)

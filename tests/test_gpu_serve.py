@@ -106,6 +106,46 @@ def test_cancel_pending_request():
         ctx.close()
 
 
+def test_cancel_running_request_and_progress():
+    """A request cancelled while it runs stops issuing paths and ends once
+    the paths in flight retire: waiting on it reports PCR_ERR_CANCELLED, its
+    fetch reports and releases it, its device memory goes back, and a request
+    that shared the wavefront with it completes unchanged.  Progress rises
+    from 0 while it runs; a finished request reports 1."""
+    from pcr_b200 import capi
+    ctx = capi.Context(device=0, queue_capacity=1 << 20)
+    try:
+        sid = ctx.load_scene_json(scene_path("cornell"), GOLDEN)
+        small = capi.render_desc(96, depth=4, samples=16, shadow=2, spectral=True, seed=3)
+        ref = ctx.render(sid, small)[0]
+        big = ctx.submit(sid, capi.render_desc(1024, depth=8, samples=1024, shadow=4, spectral=True, seed=4))
+        rid = ctx.submit(sid, small)
+        assert ctx.progress(big) == 0.0
+        seen = []
+        for _ in range(2000):
+            with pytest.raises(capi.PcrError) as e:
+                ctx.wait(big, 5)                  # drives the engine on this thread for ~5 ms
+            assert e.value.status == 6            # timed out: still running
+            seen.append(ctx.progress(big))
+            if seen[-1] > 0.01:
+                break
+        assert 0.01 < seen[-1] < 0.5 and seen == sorted(seen)
+        ctx.cancel(big)
+        with pytest.raises(capi.PcrError) as e:
+            ctx.wait(big, 60_000)
+        assert e.value.status == 7
+        with pytest.raises(capi.PcrError) as e:
+            ctx.fetch(big)
+        assert e.value.status == 7
+        ctx.wait(rid, 60_000)
+        assert ctx.progress(rid) == 1.0
+        assert np.allclose(ctx.fetch(rid)[0], ref, rtol=RTOL, atol=ATOL)
+        # the engine is idle and usable: a render after the cancel is unchanged
+        assert np.allclose(ctx.render(sid, small)[0], ref, rtol=RTOL, atol=ATOL)
+    finally:
+        ctx.close()
+
+
 def test_autotune_picks_from_grid_and_keeps_results():
     """The autotuner times trial batches over queue capacity, block size,
     issue chunk and refill cadence; the chosen tuning is one of the grid's
