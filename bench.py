@@ -57,6 +57,19 @@ NCU_DRAM_PER_UNIT = {"extend": 48.5, "shade": 408.4, "shadow": 67.6}
 # one 8-render step, divided by that step's rays / shadow rays), for the
 # issue-rate roofline below.
 NCU_INST_PER_UNIT = {"extend": 42.36, "shade": 54.61, "shadow": 31.57}
+# Algorithmic BVH-fetch bytes per ray of the batched-mesh workload's two
+# scenes: 2 x 24 B of child boxes per internal node processed plus 36 B per
+# leaf triangle tested, counted by the reference's own traversal order
+# (code/Bvh/Bvh.cpp:353-444, restated in the oracle) over every ray of the
+# reference estimator on the same scene (camera, continuation and shadow
+# rays alike; depth 8, 4 shadow rays, hero-4 spectral).  The figure does not
+# depend on the device's tree layout.  tests/test_bvh_fetch_bytes.py
+# recomputes it with the oracle and pins these values.
+BVH_BYTES_PER_RAY = {"ico59-diffuse": 223.6, "ico59-glass": 1138.9}
+# Algorithmic FP32 work of a plane test (3 dot products, 1 divide, 2
+# projections onto the quad's edges); the reference tests every plane of the
+# scene for every ray, light planes included (code/Renderer.cpp:891-949).
+PLANE_TEST_FLOPS = 25
 NCU_ISSUE = {"extend": {"issue_slots_busy": 0.658, "lanes_active": 15.5 / 32},
              "shade": {"issue_slots_busy": 0.324, "lanes_active": 23.1 / 32},
              "shadow": {"issue_slots_busy": 0.480, "lanes_active": 21.8 / 32, "l1_busy": 0.81}}
@@ -80,9 +93,9 @@ def args_():
                    help="skip the autotuner (queue size, block size, issue chunk, refill cadence)")
     p.add_argument("--serve-requests", type=int, default=2000, help="served stream length (2000: the serving config)")
     p.add_argument("--serve-rate", type=float, default=200.0)
-    p.add_argument("--mesh-batch", type=int, default=0,
-                   help="batched mesh scenes: renders per step (0: off; 32 = the mesh configuration)")
-    p.add_argument("--serve-scale", type=int, default=0,
+    p.add_argument("--mesh-batch", type=int, default=32,
+                   help="batched mesh scenes: renders per step (32 = the mesh configuration; 0: off)")
+    p.add_argument("--serve-scale", type=int, default=100,
                    help="serving at scale: requests per stream (0: off; the 1M-triangle mesh is generated on first use)")
     return p.parse_args()
 
@@ -165,17 +178,20 @@ def scene_files():
 # ------------------------------------------------------------------ reference arm
 def cpu_sample_step(scenes, batch, rows):
     """One bounded sample of the batch on the reference CPU renderer: `rows`
-    pixel rows of every request at its own depth / paths per pixel / shadow
-    rays (the reference's own castRaySpectral per path, samples = 1), all
-    host threads.  Returns (paths, seconds)."""
+    pixel rows of every request, spread evenly over its height (the centre
+    row of each of `rows` equal bands, so the sample sees the image's
+    average content, not only the ceiling and the light), at the request's
+    own depth / paths per pixel / shadow rays (the reference's own
+    castRaySpectral per path, samples = 1), all host threads.  Returns
+    (paths, seconds)."""
     from oracle import ref
     paths, secs = 0, 0.0
     for r in batch:
         o = ref.opts(r["width"], r["height"], depth=r["depth"], samples=1, shadow=r["shadow"], spectral=True,
                      seed=r["seed"])
-        h = min(rows, r["height"])
-        _, s = ref.render_hdr(scenes[r["variant"]], o, mode=1, spp=r["samples"], threads=0, rows=(0, h))
-        paths += h * r["width"] * r["samples"]
+        picked = ref.spread_rows(r["height"], rows)
+        _, s = ref.render_hdr_rows(scenes[r["variant"]], o, picked, spp=r["samples"], threads=0)
+        paths += picked.size * r["width"] * r["samples"]
         secs += s
     return paths, secs
 
@@ -205,14 +221,14 @@ def reference_arm(a):
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": a.gpus, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": 1e3 * tot_s / a.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded batch of the 10 Cornell variants)",
-        "config": {"workload": f"batch{a.renders}-uneven", "sample": f"{rows} pixel rows of each render"},
+        "config": {"workload": f"batch{a.renders}-uneven", "sample": f"{rows} pixel rows spread evenly over each render"},
         "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "reference",
-                         "sample": f"{rows} rows of each of the {a.renders} renders per step"},
+                         "sample": f"{rows} rows spread evenly over each of the {a.renders} renders per step"},
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
 
 
 # ------------------------------------------------------------------ matched image error
-def matched_run(ctx, sids, stream, a, with_cpu):
+def matched_run(ctx, sids, stream, a, with_cpu, tune, sm_mhz):
     """The Cornell configuration at matched image error: cornell.json at
     256x256, depth 4, S = 4, hero-4 spectral, Reinhard.  The target error is
     the RMSE of the reference CPU renderer's branched s = 16 image against a
@@ -270,7 +286,31 @@ def matched_run(ctx, sids, stream, a, with_cpu):
     e1.record(stream)
     torch.cuda.synchronize()
     batched_s = e0.elapsed_time(e1) / 1e3 / nb
-    out = {"config": "cornell.json 256x256, depth 4, S=4, hero-4 spectral, Reinhard",
+    fp32 = None
+    if not a.no_profile:
+        # FP32 roofline of the plane scene: the reference tests all 18 planes
+        # for every ray (camera, continuation and shadow rays); a profiled
+        # context times the two trace kernels over the same 64-image batch
+        pctx = capi.Context(device=ctx.device, profile=True, **tune)
+        psid = pctx.load_scene_json(os.path.join(REPO, "tests", "golden", "scenes", "cornell.json"),
+                                    os.path.join(REPO, "tests", "golden"))
+        ids = [pctx.submit(psid, desc(spp_star, 500 + k)) for k in range(nb)]
+        pctx.run_until_idle()
+        for i in ids:
+            pctx.fetch(i, want_hdr=False, want_rgb=False)
+        ps = pctx.stats()
+        pctx.close()
+        rays = ps["rays"] + ps["shadow_rays"]
+        t = (ps["stage_ms"]["extend"] + ps["stage_ms"]["shadow"]) / 1e3
+        mhz = sm_mhz or 1965.0
+        peak = 148 * 128 * 2 * mhz * 1e6 / 1e12
+        ach = rays * 18 * PLANE_TEST_FLOPS / t / 1e12
+        fp32 = {"kernels": "k_extend + k_shadow", "rays": rays, "flops_per_ray": 18 * PLANE_TEST_FLOPS,
+                "achieved": ach, "unit": "TFLOP/s", "peak": peak, "frac": ach / peak,
+                "peak_basis": f"148 SMs x 128 FP32 lanes x 2 (FMA) x {mhz:.0f} MHz (sampled SM clock)",
+                "flops": f"{PLANE_TEST_FLOPS} per plane test x 18 planes per ray, the reference's per-ray work",
+                "rays_per_s_in_trace_kernels": rays / t}
+    out = {"config": "cornell.json 256x256, depth 4, S=4, hero-4 spectral, Reinhard", "fp32_roofline": fp32,
            "target_rmse": eps, "target": "reference CPU branched s=16 image vs 4096-path converged image",
            "spp_star": spp_star, "gpu_rmse_at_spp_star": err, "paths_per_image": paths,
            "plain_ms_per_image": plain_s * 1e3, "plain_paths_s": paths / plain_s,
@@ -398,42 +438,104 @@ def serve_scale_run(ctx, sids, data, a):
             "mix": "10 % 2048x2048 d8 s64 S4 on 1,003,520 triangles; 90 % 64..256 squares"}
 
 
-def mesh_batch_run(ctx, stream, data, a):
+def l2_bandwidth(device):
+    """Measured L2 bandwidth of this GPU: copies between two 16 MiB buffers
+    (32 MiB in all, resident in the 126 MB L2), read + write bytes over the
+    CUDA-event time of 200 back-to-back copies, best of 3."""
+    import torch
+    n = 16 << 20
+    x = torch.empty(n, dtype=torch.uint8, device=f"cuda:{device}")
+    y = torch.empty_like(x)
+    x.fill_(1)
+    for _ in range(20):
+        y.copy_(x)
+    best = 0.0
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(200):
+            y.copy_(x)
+        e1.record()
+        torch.cuda.synchronize()
+        best = max(best, 2 * n * 200 / (e0.elapsed_time(e1) / 1e3) / 1e9)
+    return best
+
+
+def mesh_batch_run(ctx, stream, data, a, tune, hbm_peak, l2_peak):
     """Batched mesh scenes: the Cornell box with the seeded ~70k-triangle
     displaced icosphere, glass or Lambertian by seed (50/50); `n` renders
     per step, square resolution log-uniform 512..1024, depth 8, 32 paths per
     pixel, 4 shadow rays.  Device-timed like the main batched value (one
-    warm-up step, then `a.steps` steps)."""
+    warm-up step, then up to 3 steps).
+
+    BVH-fetch roofline: a profiled context renders each scene's share of the
+    batch alone; its rays (path vertices + shadow rays) times the scene's
+    algorithmic bytes per ray (BVH_BYTES_PER_RAY) over the CUDA-event time
+    of the two trace kernels (k_extend + k_shadow) is the achieved BVH-fetch
+    bandwidth, against the measured HBM copy bandwidth and the measured L2
+    bandwidth (the mesh's nodes and triangles, ~8 MB, stay in L2)."""
     import torch
 
     from pcr_b200 import capi, workloads
-    sids = {g: ctx.load_scene_json(workloads.mesh_scene(59, 21 + int(g), glass=g), data) for g in (False, True)}
+    files = {g: workloads.mesh_scene(59, 21 + int(g), glass=g) for g in (False, True)}
+    sids = {g: ctx.load_scene_json(files[g], data) for g in (False, True)}
     rng = np.random.default_rng(a.seed + 53)
     batch = []
     for _ in range(a.mesh_batch):
         side = int(round(np.exp(rng.uniform(np.log(512), np.log(1024)))))
-        batch.append((sids[bool(rng.integers(0, 2))], capi.render_desc(side, depth=8, samples=32, shadow=4,
-                                                                       spectral=True, seed=int(rng.integers(1, 2**31)))))
+        batch.append((bool(rng.integers(0, 2)), capi.render_desc(side, depth=8, samples=32, shadow=4,
+                                                                 spectral=True, seed=int(rng.integers(1, 2**31)))))
     paths = sum(d.width * d.height * d.samples for _, d in batch)
+    steps = max(1, min(a.steps, 3))
 
     def step():
-        ids = [ctx.submit(s, d) for s, d in batch]
+        ids = [ctx.submit(sids[g], d) for g, d in batch]
         ctx.run_until_idle()
         for i in ids:
             ctx.fetch(i, want_hdr=False, want_rgb=False)
     step()
+    ctx.reset_stats()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
-    for _ in range(a.steps):
+    for _ in range(steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
-    s = ev0.elapsed_time(ev1) / 1e3
+    sec = ev0.elapsed_time(ev1) / 1e3
+    st = ctx.stats()
     for v in sids.values():
         ctx.release_scene(v)
-    return {"renders": a.mesh_batch, "paths_per_step": paths, "paths_per_s": paths * a.steps / s,
-            "ms_per_step": s * 1e3 / a.steps, "triangles": 69620,
-            "config": "512..1024 squares, depth 8, 32 paths per pixel, S 4, glass / Lambertian 50/50"}
+    out = {"renders": a.mesh_batch, "paths_per_step": paths, "paths_per_s": paths * steps / sec,
+           "rays_per_s": (st["rays"] + st["shadow_rays"]) / sec, "ms_per_step": sec * 1e3 / steps, "steps": steps,
+           "triangles": 69620, "config": "512..1024 squares, depth 8, 32 paths per pixel, S 4, glass / Lambertian 50/50"}
+    if a.no_profile:
+        return out
+    roof = {}
+    for g in (False, True):
+        name = "ico59-glass" if g else "ico59-diffuse"
+        pctx = capi.Context(device=ctx.device, profile=True, **tune)
+        psid = pctx.load_scene_json(files[g], data)
+        ids = [pctx.submit(psid, d) for gg, d in batch if gg == g]
+        pctx.run_until_idle()
+        for i in ids:
+            pctx.fetch(i, want_hdr=False, want_rgb=False)
+        ps = pctx.stats()
+        pctx.close()
+        rays = ps["rays"] + ps["shadow_rays"]
+        t = (ps["stage_ms"]["extend"] + ps["stage_ms"]["shadow"]) / 1e3
+        gbs = rays * BVH_BYTES_PER_RAY[name] / t / 1e9
+        roof[name] = {"renders": len(ids), "rays": rays, "bytes_per_ray": BVH_BYTES_PER_RAY[name],
+                      "trace_ms": t * 1e3, "achieved": gbs, "unit": "GB/s", "frac_hbm": gbs / hbm_peak,
+                      "frac_l2": gbs / l2_peak if l2_peak else None,
+                      "rays_per_s_in_trace_kernels": rays / t}
+    tot_b = sum(v["rays"] * v["bytes_per_ray"] for v in roof.values())
+    tot_t = sum(v["trace_ms"] for v in roof.values()) / 1e3
+    out["bvh_fetch"] = {"kernels": "k_extend + k_shadow", "achieved": tot_b / tot_t / 1e9, "unit": "GB/s",
+                        "peak_hbm": hbm_peak, "frac_hbm": tot_b / tot_t / 1e9 / hbm_peak, "peak_l2": l2_peak,
+                        "frac_l2": tot_b / tot_t / 1e9 / l2_peak if l2_peak else None, "per_scene": roof,
+                        "bytes": "2 x 24 B per internal node processed + 36 B per leaf triangle tested, "
+                                 "reference traversal order, per ray of the reference estimator"}
+    return out
 
 
 # ------------------------------------------------------------------ CUDA arm
@@ -601,12 +703,16 @@ def main():
                                                rate=0.8 * cap, seed_off=29)
 
     serve_scale = serve_scale_run(ctx, sids, data, a) if a.serve_scale > 0 else None
-    mesh_batch = mesh_batch_run(ctx, stream, data, a) if a.mesh_batch > 0 else None
+    tune = {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")}
+    hbm_peak, hbm_kind = peaks()
+    l2_peak = l2_bandwidth(local) if not a.no_profile else None
+    mesh_batch = mesh_batch_run(ctx, stream, data, a, tune, hbm_peak, l2_peak) if a.mesh_batch > 0 else None
 
     # ---- Cornell configuration at matched image error
     matched = None
     if not a.no_matched:
-        matched = matched_run(ctx, sids, stream, a, with_cpu=(not a.no_cpu and rank == 0 and world == 1))
+        matched = matched_run(ctx, sids, stream, a, with_cpu=(not a.no_cpu and rank == 0 and world == 1), tune=tune,
+                              sm_mhz=clk.summary().get("sm_mhz"))
 
     # ---- CPU baseline (rank 0, N = 1): reference renderer on a row sample
     cpu = None
@@ -618,10 +724,17 @@ def main():
                 rows = os.cpu_count() or 8   # one row per host thread
                 pp, ss = cpu_sample_step(rscenes, batch, rows)
                 cpu = {"value": pp / ss, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                       "sample": f"{rows} pixel rows of each of the {a.renders} renders ({pp} paths, {ss:.1f} s)"}
+                       "sample": f"{rows} pixel rows spread evenly over each of the {a.renders} renders "
+                                 f"({pp} paths, {ss:.1f} s)"}
         except Exception as e:  # reported, not fatal
             cpu = {"value": None, "error": str(e)}
 
+    if roofline is not None:
+        # the path's own rooflines (bounds of the work the reference defines):
+        # BVH-fetch bytes on the mesh scenes, FP32 plane tests on cornell
+        roofline["bvh_fetch"] = (mesh_batch or {}).get("bvh_fetch")
+        roofline["fp32_issue"] = (matched or {}).get("fp32_roofline")
+        roofline["l2_peak_gbs"] = l2_peak
     if rank == 0:
         out = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,

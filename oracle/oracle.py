@@ -115,6 +115,8 @@ def lib():
             "oracle_cauchy": ([F, F, F], F),
             "oracle_dielectric": ([fp, I, F, F, fp], None),
             "oracle_hemisphere_dir": ([fp, F, F, fp], None),
+            "oracle_count_begin": ([], None),
+            "oracle_count_end": ([lp], None),
         }
         for name, (args, res) in sig.items():
             fn = getattr(L, name)
@@ -524,6 +526,20 @@ def render(sc: Scene, o: OOpts, threads: int = 1):
     lib().oracle_render(C.byref(sc.cstruct()), C.byref(o), threads, fptr(hdr),
                         rgb.ctypes.data_as(C.POINTER(C.c_ubyte)))
     return hdr, rgb
+
+
+def count_render_paths(sc: Scene, o: OOpts, spp: int, threads: int = 1) -> dict:
+    """render_paths with the reference traversal's work counted: rays
+    (sceneIntersect calls, shadow rays included), plane and sphere tests,
+    BVH internal nodes processed and leaf triangles tested."""
+    L = lib()
+    L.oracle_count_begin()
+    try:
+        render_paths(sc, o, spp, threads)
+    finally:
+        c = np.zeros(5, np.int64)
+        L.oracle_count_end(c.ctypes.data_as(C.POINTER(C.c_long)))
+    return dict(zip(["rays", "plane_tests", "sphere_tests", "bvh_nodes", "bvh_tris"], c.tolist()))
 
 
 def render_paths(sc: Scene, o: OOpts, spp: int, threads: int = 1) -> np.ndarray:

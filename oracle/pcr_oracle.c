@@ -717,7 +717,7 @@ int oracle_bvh_build(OTriangle *tris, int n, ONode *nodes)
 }
 
 /* ------------------------------------------------------------ BVH query
- * Bvh.cpp:360-377 rayAabb, :419-510 intersect.  counts (optional):
+ * Bvh.cpp:294-311 rayAabb, :353-444 intersect.  counts (optional):
  * [0] internal nodes processed, [1] leaf triangles tested. */
 static int ray_aabb(V3 o, V3 d, const float *mn, const float *mx, float segMax, float *tNear)
 {
@@ -819,11 +819,35 @@ void oracle_bvh_query(const ONode *nodes, int nNodes, const OTriangle *tris, con
     }
 }
 
+/* ------------------------------------------------------------ work counts
+ * While counting is on (oracle_count_begin .. oracle_count_end), every
+ * scene query adds to process-wide totals: [0] rays (sceneIntersect calls:
+ * camera, continuation and shadow rays alike, as the reference casts them),
+ * [1] plane tests, [2] sphere tests, [3] BVH internal nodes processed (each
+ * reads its two children's boxes), [4] leaf triangles tested.  These are the
+ * reference traversal's work, the algorithmic units of the path's rooflines. */
+static int g_counting = 0;
+static long g_counts[5];
+
+void oracle_count_begin(void)
+{
+    for (int i = 0; i < 5; i++) __atomic_store_n(&g_counts[i], 0, __ATOMIC_RELAXED);
+    __atomic_store_n(&g_counting, 1, __ATOMIC_RELEASE);
+}
+
+void oracle_count_end(long *out)
+{
+    __atomic_store_n(&g_counting, 0, __ATOMIC_RELEASE);
+    for (int i = 0; i < 5; i++) out[i] = __atomic_load_n(&g_counts[i], __ATOMIC_RELAXED);
+}
+
 /* ------------------------------------------------------------ scene query
  * Renderer::sceneIntersect (Renderer.cpp:891-949) */
 static int scene_intersect(const OScene *S, V3 o, V3 d, V3 *hit, V3 *N, int *matIdx)
 {
     float closest = FLT_MAX, t0 = 0.f;
+    long bc[2] = {0, 0};
+    const int counting = __atomic_load_n(&g_counting, __ATOMIC_RELAXED);
     for (int i = 0; i < S->nSph; i++)
     {
         if (!sphere_hit(&S->sph[i], o, d, &t0) || t0 >= closest) continue;
@@ -844,7 +868,7 @@ static int scene_intersect(const OScene *S, V3 o, V3 d, V3 *hit, V3 *N, int *mat
         V3 th, tn;
         int tm;
         float tt;
-        if (bvh_intersect(S->nodes, S->nNodes, S->tris, o, d, &th, &tn, &tm, &tt, closest, NULL))
+        if (bvh_intersect(S->nodes, S->nNodes, S->tris, o, d, &th, &tn, &tm, &tt, closest, counting ? bc : NULL))
         {
             closest = tt; *hit = th; *N = tn; *matIdx = tm;
         }
@@ -857,6 +881,15 @@ static int scene_intersect(const OScene *S, V3 o, V3 d, V3 *hit, V3 *N, int *mat
             if (!tri_hit(&S->tris[i], o, d, &th, &tn, &t0, closest) || t0 >= closest) continue;
             closest = t0; *hit = th; *N = tn; *matIdx = S->tris[i].matIdx;
         }
+        bc[1] = S->nTri;
+    }
+    if (counting)
+    {
+        __atomic_fetch_add(&g_counts[0], 1, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&g_counts[1], (long)S->nPlanes, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&g_counts[2], (long)S->nSph, __ATOMIC_RELAXED);
+        __atomic_fetch_add(&g_counts[3], bc[0], __ATOMIC_RELAXED);
+        __atomic_fetch_add(&g_counts[4], bc[1], __ATOMIC_RELAXED);
     }
     return closest < FLT_MAX;
 }

@@ -71,6 +71,8 @@ def lib():
         L.ref_render_png.restype = I
         L.ref_render_hdr.argtypes = [P, C.POINTER(RefRenderOpts), I, I, I, I, I, dp]
         L.ref_render_hdr.restype = D
+        L.ref_render_hdr_rows.argtypes = [P, C.POINTER(RefRenderOpts), I, I, ip, I, dp]
+        L.ref_render_hdr_rows.restype = D
         L.ref_scene_intersect.argtypes = [P, fp, I, ip, fp]
         L.ref_bvh_build.argtypes = [fp, I, fp, ip, ip]
         L.ref_bvh_build.restype = I
@@ -197,6 +199,23 @@ def render_hdr(scene: RefScene, o: RefRenderOpts, mode: int = 0, spp: int = 1,
     r1 = r1 or o.height
     out = np.zeros((r1 - r0, o.width, 3), np.float64)
     secs = lib().ref_render_hdr(scene.handle, C.byref(o), mode, spp, threads, r0, r1, _dp(out))
+    return out, secs
+
+
+def spread_rows(height: int, n: int) -> np.ndarray:
+    """n rows spread evenly over an image of `height` rows (the centre row of
+    each of n equal bands), so a row sample sees the image's average
+    content rather than, say, the ceiling and the light at the top."""
+    n = max(1, min(n, height))
+    return ((np.arange(n) + 0.5) * height / n).astype(np.int32)
+
+
+def render_hdr_rows(scene: RefScene, o: RefRenderOpts, rows, spp: int = 1, threads: int = 0):
+    """Paths mode (spp paths per pixel centre) over the given rows only:
+    (len(rows), W, 3) float64 linear sRGB and the loop's wall seconds."""
+    r = np.ascontiguousarray(rows, np.int32)
+    out = np.zeros((r.size, o.width, 3), np.float64)
+    secs = lib().ref_render_hdr_rows(scene.handle, C.byref(o), spp, threads, _ip(r), r.size, _dp(out))
     return out, secs
 
 

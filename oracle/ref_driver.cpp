@@ -10,7 +10,7 @@
 //   * HDR harness       -> Renderer::castRaySpectral / castRay
 //                                                      (code/Renderer.cpp:468-889)
 //   * sceneIntersect    -> Renderer::sceneIntersect    (code/Renderer.cpp:891-949)
-//   * BVH build/query   -> Bvh::build / Bvh::intersect (code/Bvh/Bvh.cpp:380-510)
+//   * BVH build/query   -> Bvh::build / Bvh::intersect (code/Bvh/Bvh.cpp:122-325, 353-444)
 //   * stage functions   -> RGBToSpectrum / CIE / ToneMap / Optics headers
 //
 // The private members of Renderer are reached by compiling this one file
@@ -426,6 +426,54 @@ double ref_render_hdr(void *h, const RefRenderOpts *o, int mode, int spp, int th
                     }
                     double *px = out + ((size_t)(i - rowBegin) * o->width + j) * 3;
                     px[0] = acc[0]; px[1] = acc[1]; px[2] = acc[2];
+                }
+            }
+        });
+    }
+    for (auto &th : pool) th.join();
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// ref_render_hdr in paths mode (spp paths per pixel centre, samples = 1)
+// over an explicit list of rows, e.g. a sample spread evenly over the image;
+// the threads share the list.  out holds nrows x width x 3 (linear sRGB).
+double ref_render_hdr_rows(void *h, const RefRenderOpts *o, int spp, int threads, const int *rows, int nrows,
+                           double *out)
+{
+    auto &s = ((RefScene *)h)->data;
+    NumGen::setSeed(o->seed);
+    pcr_ref_numgen_reset();
+    const int nThreads = threads > 0 ? threads : (int)std::thread::hardware_concurrency();
+    auto t0 = std::chrono::steady_clock::now();
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nThreads; t++)
+    {
+        pool.emplace_back([&, t]() {
+            Renderer r(o->width, o->height, o->depth, 1, o->shadow);
+            r.useMIS = o->mis; r.useRussian = o->russian; r.useStratified = o->stratified;
+            r.useSpectral = o->spectral; r.heroSamples = o->hero;
+            float totalLightArea;
+            preparePlanes(r, s, totalLightArea);
+            for (int k = t; k < nrows; k += nThreads)
+            {
+                for (int j = 0; j < o->width; j++)
+                {
+                    double acc[3] = {0, 0, 0};
+                    for (int q = 0; q < spp; q++)
+                    {
+                        Vec3f c = cameraSample(r, s, o, totalLightArea, rows[k], j, false);
+                        for (int ch = 0; ch < 3; ch++) acc[ch] += c[ch];
+                    }
+                    for (int ch = 0; ch < 3; ch++) acc[ch] /= spp;
+                    if (o->spectral)
+                    {
+                        const double X = acc[0], Y = acc[1], Z = acc[2];
+                        acc[0] = 3.2404542 * X - 1.5371385 * Y - 0.4985314 * Z;
+                        acc[1] = -0.9692660 * X + 1.8760108 * Y + 0.0415560 * Z;
+                        acc[2] = 0.0556434 * X - 0.2040259 * Y + 1.0572252 * Z;
+                    }
+                    double *px = out + ((size_t)k * o->width + j) * 3;
+                    for (int ch = 0; ch < 3; ch++) px[ch] = acc[ch];
                 }
             }
         });

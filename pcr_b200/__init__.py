@@ -6,8 +6,10 @@ C ABI of include/pcr_cuda.h.
     sid = ctx.load_scene_json("Scenes/cornell.json")
     hdr, rgb8, stats = ctx.render(sid, capi.render_desc(256, depth=4, samples=16, shadow=4))
 
-`pcr_b200.renderer.Renderer` mirrors the reference renderer's surface
-(constructor, quality knobs, render(scene, start, outputDir) writing the PNG).
+The reference renderer's C++ surface (constructor, quality knobs,
+render(scene, start, outputDir) writing the PNG) is `CudaRenderer` in
+pcr_b200/csrc/cuda_renderer.h, built over the same C ABI; the `pcr-render`
+CLI in pcr_b200/lib takes the reference CLI's flags.
 """
 from . import capi  # noqa: F401
 
