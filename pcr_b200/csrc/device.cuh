@@ -175,7 +175,7 @@ __device__ __forceinline__ bool blocks_at(float3 o, float3 d, float t, double li
 }
 
 // One child box of a 4-wide node with the reference's slab arithmetic
-// (code/Bvh/Bvh.cpp:360-377), branch-free: the reference returns at the
+// (code/Bvh/Bvh.cpp:294-311), branch-free: the reference returns at the
 // first axis where tmin > tmax, and since tmin only grows and tmax only
 // shrinks, testing once after all three axes gives the same answer.  NaN
 // lanes are ignored the way std::max/std::min ignore a NaN second argument.
