@@ -438,29 +438,6 @@ def serve_scale_run(ctx, sids, data, a):
             "mix": "10 % 2048x2048 d8 s64 S4 on 1,003,520 triangles; 90 % 64..256 squares"}
 
 
-def l2_bandwidth(device):
-    """Measured L2 bandwidth of this GPU: copies between two 16 MiB buffers
-    (32 MiB in all, resident in the 126 MB L2), read + write bytes over the
-    CUDA-event time of 200 back-to-back copies, best of 3."""
-    import torch
-    n = 16 << 20
-    x = torch.empty(n, dtype=torch.uint8, device=f"cuda:{device}")
-    y = torch.empty_like(x)
-    x.fill_(1)
-    for _ in range(20):
-        y.copy_(x)
-    best = 0.0
-    for _ in range(3):
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
-        for _ in range(200):
-            y.copy_(x)
-        e1.record()
-        torch.cuda.synchronize()
-        best = max(best, 2 * n * 200 / (e0.elapsed_time(e1) / 1e3) / 1e9)
-    return best
-
-
 def mesh_batch_run(ctx, stream, data, a, tune, hbm_peak, l2_peak):
     """Batched mesh scenes: the Cornell box with the seeded ~70k-triangle
     displaced icosphere, glass or Lambertian by seed (50/50); `n` renders
@@ -473,7 +450,7 @@ def mesh_batch_run(ctx, stream, data, a, tune, hbm_peak, l2_peak):
     algorithmic bytes per ray (BVH_BYTES_PER_RAY) over the CUDA-event time
     of the two trace kernels (k_extend + k_shadow) is the achieved BVH-fetch
     bandwidth, against the measured HBM copy bandwidth and the measured L2
-    bandwidth (the mesh's nodes and triangles, ~8 MB, stay in L2)."""
+    L2 read bandwidth (the mesh's nodes and triangles, ~8 MB, stay in L2)."""
     import torch
 
     from pcr_b200 import capi, workloads
@@ -705,7 +682,9 @@ def main():
     serve_scale = serve_scale_run(ctx, sids, data, a) if a.serve_scale > 0 else None
     tune = {k: st[k] for k in ("queue_capacity", "block_size", "chunk_paths", "regen_every")}
     hbm_peak, hbm_kind = peaks()
-    l2_peak = l2_bandwidth(local) if not a.no_profile else None
+    # measured L2 read bandwidth (the library's probe: a 32 MiB buffer read
+    # 400 times with L1-bypassing loads), best of 3
+    l2_peak = max(ctx.l2_bandwidth(32 << 20, 400) for _ in range(3)) if not a.no_profile else None
     mesh_batch = mesh_batch_run(ctx, stream, data, a, tune, hbm_peak, l2_peak) if a.mesh_batch > 0 else None
 
     # ---- Cornell configuration at matched image error

@@ -244,6 +244,13 @@ typedef struct {
     int32_t queue_capacity, block_size, chunk_paths, regen_every;
 } pcr_engine_stats;
 pcr_status pcr_engine_stats_get(pcr_ctx *ctx, pcr_engine_stats *out);
+/* Measures the device's L2 read bandwidth (GB/s): a kernel reads an
+ * L2-resident buffer of `bytes` (1..96 MiB; 32 MiB fits the 126 MB L2 of a
+ * B200 with room to spare) `reps` times with loads that bypass L1.  The
+ * denominator of the BVH-fetch roofline's L2 fraction: a mesh's nodes and
+ * triangles (a few MB to ~60 MB) stay in L2 while rays traverse it.  No
+ * reference counterpart (measurement only). */
+pcr_status pcr_l2_bandwidth(pcr_ctx *ctx, int64_t bytes, int32_t reps, double *gbs);
 pcr_status pcr_engine_stats_reset(pcr_ctx *ctx);
 /* Picks queue capacity (512K..4M paths in flight), block size, chunk and
  * refill cadence by timing short trial batches of the given requests; stores

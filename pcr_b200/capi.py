@@ -25,7 +25,7 @@ EXPORTS = [
     "pcr_scene_upload", "pcr_scene_load_json", "pcr_host_scene_load", "pcr_host_scene_free",
     "pcr_fit_sigmoid", "pcr_lut_build", "pcr_scene_release", "pcr_scene_bytes", "pcr_render", "pcr_render_noalloc",
     "pcr_submit", "pcr_run_until_idle", "pcr_serve_start", "pcr_serve_stop", "pcr_poll", "pcr_wait",
-    "pcr_fetch", "pcr_cancel", "pcr_progress", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
+    "pcr_fetch", "pcr_cancel", "pcr_progress", "pcr_l2_bandwidth", "pcr_engine_stats_get", "pcr_engine_stats_reset", "pcr_autotune",
     "pcr_trace_closest", "pcr_trace_bvh", "pcr_trace_shadow", "pcr_bvh_build", "pcr_eval_stage",
     "pcr_tonemap", "pcr_router_create", "pcr_router_destroy", "pcr_router_scene_load_json", "pcr_router_serve_start",
     "pcr_router_serve_stop", "pcr_router_submit", "pcr_router_wait", "pcr_router_fetch", "pcr_router_load",
@@ -153,6 +153,7 @@ def load_library():
         "pcr_fetch": [P, C.c_int64, fp, up, C.POINTER(RenderStats)],
         "pcr_cancel": [P, C.c_int64],
         "pcr_progress": [P, C.c_int64, C.POINTER(C.c_double)],
+        "pcr_l2_bandwidth": [P, C.c_int64, C.c_int32, C.POINTER(C.c_double)],
         "pcr_engine_stats_get": [P, C.POINTER(EngineStats)],
         "pcr_engine_stats_reset": [P],
         "pcr_autotune": [P, ip, C.POINTER(RenderDesc), C.c_int32, ip],
@@ -391,6 +392,12 @@ class Context:
 
     def cancel(self, rid: int) -> None:
         _check(self.L.pcr_cancel(self.h, rid))
+
+    def l2_bandwidth(self, nbytes: int = 32 << 20, reps: int = 400) -> float:
+        """Measured L2 read bandwidth of this context's device, GB/s."""
+        g = C.c_double()
+        _check(self.L.pcr_l2_bandwidth(self.h, nbytes, reps, C.byref(g)))
+        return g.value
 
     def progress(self, rid: int) -> float:
         f = C.c_double()

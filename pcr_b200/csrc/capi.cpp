@@ -276,6 +276,14 @@ pcr_status pcr_cancel(pcr_ctx* ctx, pcr_request_id id)
     return guard([&] { E(ctx).cancel(id); });
 }
 
+pcr_status pcr_l2_bandwidth(pcr_ctx* ctx, int64_t bytes, int32_t reps, double* gbs)
+{
+    return guard([&] {
+        if (!gbs) throw pcr::PcrError(PCR_ERR_INVALID, "null argument");
+        *gbs = E(ctx).l2_bandwidth(bytes, reps);
+    });
+}
+
 pcr_status pcr_progress(pcr_ctx* ctx, pcr_request_id id, double* fraction)
 {
     return guard([&] {

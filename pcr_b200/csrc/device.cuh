@@ -113,10 +113,21 @@ __device__ __forceinline__ bool plane_hit(const DPlane& p, float3 o, float3 d, f
     // makes s negative (|a / uu| stays far above the smallest subnormal for
     // any |u| < 1e12).
     if (a < -1e-20f || b < -1e-20f) return false;
-    if (a * rcp_approx(u.w) > kUp || b * rcp_approx(v.w) > kUp) return false;
-    float s = div(a, u.w);
-    float q = div(b, v.w);
-    if (s > 1.f || s < 0.f || q > 1.f || q < 0.f) return false;
+    const float sa = a * rcp_approx(u.w), qa = b * rcp_approx(v.w);
+    if (sa > kUp || qa > kUp) return false;
+    // s and q only feed the range test: an estimate inside (0, 1) by more
+    // than its error margin (a, b > 1e-30, far from underflow) decides it
+    // as the correctly rounded quotient would, so only estimates near 0 or
+    // 1 are divided exactly
+    const bool s_in = a > 1e-30f && sa < kDown, q_in = b > 1e-30f && qa < kDown;
+    if (!s_in) {
+        const float sx = div(a, u.w);
+        if (sx > 1.f || sx < 0.f) return false;
+    }
+    if (!q_in) {
+        const float qx = div(b, v.w);
+        if (qx > 1.f || qx < 0.f) return false;
+    }
     return true;
 }
 
@@ -335,13 +346,12 @@ __device__ __forceinline__ bool group_may_hit(float4 lo, float4 hi, float3 o, fl
     return tmin <= tmax;
 }
 
-// Renderer::sceneIntersect (code/Renderer.cpp:891-949): spheres, then planes
-// (light planes first), then the triangle BVH; first-tested wins ties.
-// Returns the primitive code; t and barycentrics through refs.
-__device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, float3 d, float tmax, float& t, float& hu,
-                                                  float& hv)
+// The analytic part of Renderer::sceneIntersect (code/Renderer.cpp:891-949):
+// spheres, then planes (light planes first); first-tested wins ties.
+// Returns the primitive code (kPrimNone on a miss) with `closest` lowered to
+// its t.
+__device__ __forceinline__ uint32_t scene_analytic(const DScene& S, float3 o, float3 d, float& closest)
 {
-    float closest = tmax;
     uint32_t prim = kPrimNone;
     for (int i = 0; i < S.n_spheres; i++) {
         float t0;
@@ -366,6 +376,16 @@ __device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, flo
             }
         }
     }
+    return prim;
+}
+
+// Renderer::sceneIntersect: the analytic primitives, then the triangle BVH.
+// Returns the primitive code; t and barycentrics through refs.
+__device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, float3 d, float tmax, float& t, float& hu,
+                                                  float& hv)
+{
+    float closest = tmax;
+    uint32_t prim = scene_analytic(S, o, d, closest);
     int tri = bvh4_closest<false>(S, o, d, closest, hu, hv, nullptr);
     if (tri >= 0) prim = kPrimTri | (uint32_t)tri;
     t = closest;
@@ -383,23 +403,27 @@ __device__ __forceinline__ uint32_t scene_closest(const DScene& S, float3 o, flo
 // with t), so the answer is the closest-hit test's.  Scenes with emissive
 // triangles, or with more emissive spheres or planes than the scene record
 // lists, take the closest-hit route.
-__device__ __forceinline__ bool scene_blocked(const DScene& S, const DMaterial* mats, float3 o, float3 d, float tmax,
-                                              double lim)
+// The part of the shadow query before the triangle BVH: kShadowBlocked or
+// kShadowLit when that already decides it (the closest-hit route of scenes
+// with emissive triangles is decided here in full), else kShadowWalk with
+// `bound` set for an any-hit walk of the BVH.
+constexpr int kShadowLit = 0, kShadowBlocked = 1, kShadowWalk = 2;
+__device__ __forceinline__ int scene_blocked_analytic(const DScene& S, const DMaterial* mats, float3 o, float3 d,
+                                                      float tmax, double lim, float& bound)
 {
-    float t, hu, hv;
     if (S.emissive_tris || S.n_emit_spheres < 0 || S.n_emit_planes < 0) {
-        t = FLT_MAX;
+        float t = FLT_MAX, hu, hv;
         const uint32_t prim = scene_closest(S, o, d, tmax, t, hu, hv);
-        if ((prim & kPrimKindMask) == kPrimNone) return false;
+        if ((prim & kPrimKindMask) == kPrimNone) return kShadowLit;
         const uint32_t kind = prim & kPrimKindMask, pidx = prim & kPrimIndexMask;
         int mi;
         if (kind == kPrimSphere) mi = S.spheres[pidx].mat.x;
         else if (kind == kPrimPlane) mi = __float_as_int(S.planes[pidx].o_mat.w);
         else mi = __float_as_int(S.tris[pidx].e1_mat.w);
-        if (mats[S.mat_base + mi].flags & kMatEmissive) return false;
-        return blocks_at(o, d, t, lim);
+        if (mats[S.mat_base + mi].flags & kMatEmissive) return kShadowLit;
+        return blocks_at(o, d, t, lim) ? kShadowBlocked : kShadowLit;
     }
-    float bound = tmax;
+    bound = tmax;
     for (int k = 0; k < S.n_emit_spheres; k++) {
         float t0;
         if (sphere_hit(S.spheres[S.emit_spheres[k]], o, d, t0) && t0 < bound) bound = t0;
@@ -411,7 +435,7 @@ __device__ __forceinline__ bool scene_blocked(const DScene& S, const DMaterial* 
     for (int i = 0; i < S.n_spheres; i++) {
         float t0;
         if (sphere_hit(S.spheres[i], o, d, t0) && t0 < bound) {
-            if (blocks_at(o, d, t0, lim)) return true;
+            if (blocks_at(o, d, t0, lim)) return kShadowBlocked;
             bound = t0;
         }
     }
@@ -423,11 +447,20 @@ __device__ __forceinline__ bool scene_blocked(const DScene& S, const DMaterial* 
         for (int i = first; i < first + count; i++) {
             float t0;
             if (plane_hit(S.splanes[i], o, d, bound, t0) && t0 < bound) {
-                if (blocks_at(o, d, t0, lim)) return true;
+                if (blocks_at(o, d, t0, lim)) return kShadowBlocked;
                 bound = t0;
             }
         }
     }
+    return S.n_nodes > 0 ? kShadowWalk : kShadowLit;
+}
+
+__device__ __forceinline__ bool scene_blocked(const DScene& S, const DMaterial* mats, float3 o, float3 d, float tmax,
+                                              double lim)
+{
+    float bound = tmax, hu, hv;
+    const int r = scene_blocked_analytic(S, mats, o, d, tmax, lim, bound);
+    if (r != kShadowWalk) return r == kShadowBlocked;
     return bvh4_closest<false, true>(S, o, d, bound, hu, hv, nullptr, lim) == -2;
 }
 
@@ -480,11 +513,19 @@ __device__ __forceinline__ float wyman(float l, float mu, float s1, float s2)
     // amplified past 1e-5 there
     return (float)exp((double)mul(mul(-0.5f, t), t));
 }
+// x-bar with the reference's float operations: its negative lobe cancels the
+// other two near 501 nm, where the float evaluation's own rounding is a
+// sizeable part of the (small) result
+__device__ __forceinline__ float cmf_x(float l)
+{
+    using namespace ex;
+    return sub(add(mul(0.362f, wyman(l, 442.0f, 0.0624f, 0.0374f)), mul(1.056f, wyman(l, 599.8f, 0.0264f, 0.0323f))),
+               mul(0.065f, wyman(l, 501.1f, 0.0490f, 0.0382f)));
+}
 __device__ __forceinline__ float3 cmf(float l)
 {
     using namespace ex;
-    float x = sub(add(mul(0.362f, wyman(l, 442.0f, 0.0624f, 0.0374f)), mul(1.056f, wyman(l, 599.8f, 0.0264f, 0.0323f))),
-                  mul(0.065f, wyman(l, 501.1f, 0.0490f, 0.0382f)));
+    float x = cmf_x(l);
     float y = add(mul(0.821f, wyman(l, 568.8f, 0.0213f, 0.0247f)), mul(0.286f, wyman(l, 530.9f, 0.0613f, 0.0322f)));
     float z = add(mul(1.217f, wyman(l, 437.0f, 0.0845f, 0.0278f)), mul(0.681f, wyman(l, 459.0f, 0.0385f, 0.0725f)));
     return make_float3(x, y, z);

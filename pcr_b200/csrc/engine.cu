@@ -1766,6 +1766,59 @@ void Engine::eval_stage(int what, const float* params, const float* in, int64_t 
     CK(cudaStreamSynchronize(stream_));
 }
 
+// ---------------------------------------------------------------- L2 bandwidth
+// Reads an L2-resident buffer `reps` times with loads that bypass L1
+// (ld.global.cg), four 16-byte loads in flight per thread per step; each
+// thread writes its sum so the loads are kept.
+__global__ void __launch_bounds__(256) k_l2_read(const float4* __restrict__ buf, long long n4, int reps, float* out)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    float acc = 0.f;
+    for (int r = 0; r < reps; r++) {
+        long long i = t0;
+        for (; i + 3 * stride < n4; i += 4 * stride) {
+            const float4 a = __ldcg(buf + i), b = __ldcg(buf + i + stride), c = __ldcg(buf + i + 2 * stride),
+                         d = __ldcg(buf + i + 3 * stride);
+            acc += (a.x + b.y) + (c.z + d.w);
+        }
+        for (; i < n4; i += stride) acc += __ldcg(buf + i).x;
+    }
+    out[t0] = acc;
+}
+
+double Engine::l2_bandwidth(int64_t bytes, int reps)
+{
+    std::lock_guard<std::mutex> g(run_mu_);
+    CK(cudaSetDevice(device_));
+    if (bytes < (1 << 20) || bytes > (int64_t)96 << 20 || reps < 1)
+        throw PcrError(PCR_ERR_INVALID, "l2 bandwidth probe: 1..96 MiB and at least one pass");
+    const int block = 256, grid = sms_ * 8;
+    const int64_t n4 = bytes / 16;
+    float4* buf = nullptr;
+    float* out = nullptr;
+    CK(cudaMallocFromPoolAsync(&buf, n4 * 16, pool_, stream_));
+    CK(cudaMallocFromPoolAsync(&out, (size_t)grid * block * sizeof(float), pool_, stream_));
+    CK(cudaMemsetAsync(buf, 0, n4 * 16, stream_));
+    k_l2_read<<<grid, block, 0, stream_>>>(buf, n4, 2, out);  // warm: brings the buffer into L2
+    cudaEvent_t a, z;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&z));
+    CK(cudaEventRecord(a, stream_));
+    k_l2_read<<<grid, block, 0, stream_>>>(buf, n4, reps, out);
+    CK(cudaEventRecord(z, stream_));
+    CK(cudaGetLastError());
+    CK(cudaEventSynchronize(z));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, a, z));
+    cudaEventDestroy(a);
+    cudaEventDestroy(z);
+    CK(cudaFreeAsync(buf, stream_));
+    CK(cudaFreeAsync(out, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return (double)n4 * 16 * reps / (ms * 1e-3) / 1e9;
+}
+
 // ---------------------------------------------------------------- stats / tuning
 void Engine::stats(pcr_engine_stats* o)
 {

@@ -97,6 +97,7 @@ public:
     void build_bvh(const pcr_triangle* tris, int n, std::vector<pcr_bvh_node>& nodes, std::vector<int32_t>& order);
     void tonemap(const float* hdr, int width, int height, int aces_tm, int denoise, uint8_t* rgb8);
     void eval_stage(int what, const float* params, const float* in, int64_t n, float* out);
+    double l2_bandwidth(int64_t bytes, int reps);
 
     void stats(pcr_engine_stats* out);
     void reset_stats();

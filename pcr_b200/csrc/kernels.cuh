@@ -133,11 +133,14 @@ struct XyzWeights {
 // the Wyman-Sloan-Shirley lobes (code/Includes/CIE.h:27-53, their float
 // constants) evaluated in double at the exact grid wavelength, then rounded
 // once; the lookup's fraction comes from one fused multiply-add of the exact
-// difference lambda - kCmfLo, so the only error left is the interpolation's.
-// Against the reference's float evaluation (singleLambdaXYZ) the result
-// stays below 1e-5 relative, or 1e-7 absolute near zero, over 380..720 nm
-// (x-bar near 508 nm, where its lobes cancel, is the tightest point).
-constexpr float kCmfLo = 380.f, kCmfHi = 720.f;
+// difference lambda - kCmfLo, so the only error left is the interpolation's,
+// below 2e-6 of each value.  In [kCmfXLo, kCmfXHi] x-bar's lobes cancel and
+// the reference's own float evaluation (singleLambdaXYZ) carries rounding of
+// up to 3e-5 of the result, which no smooth table follows; there x-bar is
+// evaluated with the reference's float operations instead (xyz_weights).  Against the
+// reference the result then stays below 1e-5 relative (1e-7 absolute near
+// zero) over 380..720 nm.
+constexpr float kCmfLo = 380.f, kCmfHi = 720.f, kCmfXLo = 495.f, kCmfXHi = 508.f;
 constexpr int kCmfPerNm = 80;
 constexpr int kCmfEntries = 340 * kCmfPerNm + 1;  // (kCmfHi - kCmfLo) * kCmfPerNm + 1
 __device__ __forceinline__ double wyman_d(double l, float mu, float s1, float s2)
@@ -169,6 +172,7 @@ __device__ __forceinline__ float3 cmf_lut(const float4* __restrict__ table, floa
     const float4 a = table[i], b = table[i + 1];
     return make_float3(a.x + (b.x - a.x) * f, a.y + (b.y - a.y) * f, a.z + (b.z - a.z) * f);
 }
+__device__ __forceinline__ bool in_cmf_x_window(float l) { return l >= kCmfXLo && l <= kCmfXHi; }
 
 __device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, int nch, float wN, float xyz_scale,
                                                const float4* cmf_table)
@@ -181,14 +185,26 @@ __device__ __noinline__ XyzWeights xyz_weights(bool spectral, const float* lam, 
         W.w[3] = make_float3(0.f, 0.f, 0.f);
         return W;
     }
+    const float s = xyz_scale * wN;
+    int kx = -1;  // the wavelength in x-bar's exact window, if any
     for (int k = 0; k < 4; k++) {
         if (k < nch) {
             float3 c = cmf_lut(cmf_table, lam[k]);
-            const float s = xyz_scale * wN;
+            if (in_cmf_x_window(lam[k])) kx = k;
             W.w[k] = make_float3(c.x * s, c.y * s, c.z * s);
         } else {
             W.w[k] = make_float3(0.f, 0.f, 0.f);
         }
+    }
+    // a path's wavelengths lie 300/N nm apart (75 at N = 4) and the window is
+    // 13 nm wide, so at most one of them is in it: one exact evaluation per
+    // lane, outside the loop, keeps a warp from running it up to four times
+    if (kx >= 0) {
+        const float x = cmf_x(lam[kx]) * s;
+        if (kx == 0) W.w[0].x = x;
+        else if (kx == 1) W.w[1].x = x;
+        else if (kx == 2) W.w[2].x = x;
+        else W.w[3].x = x;
     }
     return W;
 }
