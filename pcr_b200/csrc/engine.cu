@@ -120,7 +120,6 @@ Engine::Engine(const pcr_ctx_opts* o)
     CK(cudaSetDevice(device_));
     CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-    CK(cudaStreamCreateWithFlags(&copy_stream_, cudaStreamNonBlocking));
     xyz_scale_ = (700.f - 400.f) / host_ybar_integral();
     slot_owner_.assign(kMaxActive, -1);
     scenes_.reserve(256);
@@ -158,9 +157,11 @@ Engine::~Engine()
         if (r.ev_ready) cudaEventDestroy(r.ev_ready);
     }
     cudaStreamSynchronize(stream_);
-    cudaStreamSynchronize(copy_stream_);
-    if (staging_) cudaFreeHost(staging_);
-    cudaStreamDestroy(copy_stream_);
+    for (Staging& st : staging_idle_) {
+        cudaStreamSynchronize(st.stream);
+        if (st.buf) cudaFreeHost(st.buf);
+        cudaStreamDestroy(st.stream);
+    }
     for (auto& s : scenes_)
         for (void* p : s.allocs) cudaFree(p);
     free_buffers();
@@ -702,6 +703,13 @@ void Engine::ensure_shadow_capacity(int shadow_samples)
 {
     const int64_t need = (int64_t)queue_cap_ * std::max(8, shadow_samples);
     if (need <= shadow_cap_) return;
+    // shadow records are indexed with 32-bit ints (and 2^31 records would
+    // take ~100 GB): the product must stay below 2^31
+    if (need > (int64_t)INT32_MAX)
+        throw PcrError(PCR_ERR_INVALID, std::to_string(shadow_samples) + " shadow samples per hit at " +
+                                            std::to_string(tune_.queue_capacity) +
+                                            " paths in flight exceed the 2^31-record shadow queue; use a smaller "
+                                            "queue capacity");
     CK(cudaStreamSynchronize(stream_));
     for (float4* p : {sq_.o, sq_.d, sq_.c}) {
         auto it = std::find(qallocs_.begin(), qallocs_.end(), (void*)p);
@@ -986,30 +994,64 @@ void Engine::release_cancelled(Request& r)
     r.t_ready = std::chrono::steady_clock::now();
 }
 
-// Copies a resolved request's images to caller host buffers through one
-// reusable pinned staging buffer on the copy stream (ordered after the
-// resolve by the request's event), then frees its device images.
+// A pinned staging buffer of at least `bytes` with its copy stream: an idle
+// one when one is large enough, else an idle one grown, else a new one.
+Engine::Staging Engine::take_staging(size_t bytes)
+{
+    Staging st;
+    {
+        std::lock_guard<std::mutex> g(staging_mu_);
+        int pick = -1;
+        for (int k = 0; k < (int)staging_idle_.size(); k++) {
+            const size_t have = staging_idle_[k].bytes;
+            if (have >= bytes && (pick < 0 || have < staging_idle_[pick].bytes)) pick = k;
+        }
+        if (pick < 0 && !staging_idle_.empty()) pick = 0;
+        if (pick >= 0) {
+            st = staging_idle_[pick];
+            staging_idle_.erase(staging_idle_.begin() + pick);
+        }
+    }
+    if (!st.stream) CK(cudaStreamCreateWithFlags(&st.stream, cudaStreamNonBlocking));
+    if (st.bytes < bytes) {
+        if (st.buf) CK(cudaFreeHost(st.buf));
+        st.buf = nullptr;
+        st.bytes = 0;
+        CK(cudaMallocHost(&st.buf, bytes));
+        st.bytes = bytes;
+    }
+    return st;
+}
+
+void Engine::give_staging(const Staging& st)
+{
+    std::lock_guard<std::mutex> g(staging_mu_);
+    staging_idle_.push_back(st);
+}
+
+// Copies a resolved request's images to caller host buffers through a
+// pinned staging buffer on its own copy stream (ordered after the resolve by
+// the request's event), then frees its device images.
 void Engine::copy_out(Request& r, float* hdr, uint8_t* rgb)
 {
-    std::lock_guard<std::mutex> g(copy_mu_);
     const int64_t px = (int64_t)r.desc.width * r.desc.height;
-    const size_t need = (size_t)px * 3 * (sizeof(float) + 1);
-    if ((hdr || rgb) && need > staging_bytes_) {
-        if (staging_) CK(cudaFreeHost(staging_));
-        staging_ = nullptr;
-        CK(cudaMallocHost(&staging_, need));
-        staging_bytes_ = need;
-    }
-    CK(cudaStreamWaitEvent(copy_stream_, r.ev_ready, 0));
-    float* sh = reinterpret_cast<float*>(staging_);
-    uint8_t* sr = staging_ ? staging_ + px * 3 * sizeof(float) : nullptr;
-    if (hdr) CK(cudaMemcpyAsync(sh, r.d_hdr, px * 3 * sizeof(float), cudaMemcpyDeviceToHost, copy_stream_));
-    if (rgb) CK(cudaMemcpyAsync(sr, r.d_rgb, px * 3, cudaMemcpyDeviceToHost, copy_stream_));
-    CK(cudaFreeAsync(r.d_hdr, copy_stream_));
-    CK(cudaFreeAsync(r.d_rgb, copy_stream_));
+    const size_t need = (hdr || rgb) ? (size_t)px * 3 * (sizeof(float) + 1) : 0;
+    struct Hold {  // hands the buffer back on every exit path
+        Engine* e;
+        Staging st;
+        ~Hold() { e->give_staging(st); }
+    } hold{this, take_staging(need)};
+    const Staging& st = hold.st;
+    CK(cudaStreamWaitEvent(st.stream, r.ev_ready, 0));
+    float* sh = reinterpret_cast<float*>(st.buf);
+    uint8_t* sr = st.buf ? st.buf + px * 3 * sizeof(float) : nullptr;
+    if (hdr) CK(cudaMemcpyAsync(sh, r.d_hdr, px * 3 * sizeof(float), cudaMemcpyDeviceToHost, st.stream));
+    if (rgb) CK(cudaMemcpyAsync(sr, r.d_rgb, px * 3, cudaMemcpyDeviceToHost, st.stream));
+    CK(cudaFreeAsync(r.d_hdr, st.stream));
+    CK(cudaFreeAsync(r.d_rgb, st.stream));
     r.d_hdr = nullptr;
     r.d_rgb = nullptr;
-    CK(cudaStreamSynchronize(copy_stream_));
+    CK(cudaStreamSynchronize(st.stream));
     if (hdr) std::memcpy(hdr, sh, px * 3 * sizeof(float));
     if (rgb) std::memcpy(rgb, sr, px * 3);
 }
@@ -1865,12 +1907,17 @@ void Engine::autotune(const int32_t* scenes, const pcr_render_desc* descs, int n
 {
     struct Cand { int q, b, c, r; };
     std::vector<Cand> cands;
-    // up to 4M paths in flight: 16M path slots, and S = 64 shadow rays per
-    // slot still fit the 2^31-entry shadow queue
-    for (int q : {1 << 19, 1 << 20, 1 << 21, 1 << 22})
+    // up to 16M paths in flight (64M path slots; about 40 GB of path and
+    // shadow queues at 8 shadow rays per hit).  Shadow records are indexed
+    // with 32-bit ints, so a capacity whose slots times the sample requests'
+    // shadow rays per hit reach 2^31 is skipped.
+    int max_shadow = 8;
+    for (int i = 0; i < n; i++) max_shadow = std::max(max_shadow, descs[i].shadow_samples);
+    for (int q : {1 << 19, 1 << 20, 1 << 21, 1 << 22, 1 << 23, 1 << 24})
         for (int b : {64, 128, 256})
             for (int c : {1 << 14, 1 << 16})
-                for (int r : {1, 2}) cands.push_back({q, b, c, r});
+                for (int r : {1, 2})
+                    if ((int64_t)q * 4 * max_shadow <= (int64_t)INT32_MAX) cands.push_back({q, b, c, r});
     EngineTuning best = tune_;
     double best_ms = 1e30;
     cudaEvent_t a, z;

@@ -133,10 +133,18 @@ private:
     int device_ = 0;
     int sms_ = 148;
     cudaStream_t stream_ = nullptr;
-    cudaStream_t copy_stream_ = nullptr;   // result copies, ordered by request events
-    std::mutex copy_mu_;
-    uint8_t* staging_ = nullptr;           // pinned, reused across fetches
-    size_t staging_bytes_ = 0;
+    // Result copies: pinned staging buffers, each with its own copy stream,
+    // kept idle between fetches.  A fetch takes one (or makes one), so
+    // fetches from several threads copy at the same time.
+    struct Staging {
+        uint8_t* buf = nullptr;
+        size_t bytes = 0;
+        cudaStream_t stream = nullptr;
+    };
+    std::mutex staging_mu_;
+    std::vector<Staging> staging_idle_;
+    Staging take_staging(size_t bytes);
+    void give_staging(const Staging& s);
     EngineTuning tune_;
     bool use_graph_ = true, profile_ = false;
     int64_t budget_ = 40ll << 30;
