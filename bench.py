@@ -43,20 +43,22 @@ UNIT = "paths/s"
 HBM_FALLBACK = 6650.0
 # DRAM bytes (read + write) per unit of each wavefront kernel, measured with
 # ncu (dram__bytes_read.sum + dram__bytes_write.sum over every launch of one
-# 8-render step, divided by that step's rays / shadow rays; the summary and
-# command are kept in the profiles directory).  Traffic grows in proportion to
-# the units, so a launch's traffic is this figure times its units.
-NCU_DRAM_PER_UNIT = {"extend": 48.5, "shade": 408.4, "shadow": 67.6}
+# 8-render step, divided by that step's rays / shadow rays; each launch
+# replayed alone with a cold L2; the summary and command are kept in the
+# profiles directory).  Traffic grows in proportion to the units, so a
+# launch's traffic is this figure times its units.
+NCU_DRAM_PER_UNIT = {"extend": 61.0, "shade": 514.9, "shadow": 84.2}
+# Warp instructions per unit (smsp__inst_executed.sum over the same
+# launches, divided by the same units), for the issue-rate roofline below.
+NCU_INST_PER_UNIT = {"extend": 48.25, "shade": 71.65, "shadow": 36.84}
 # Issue-rate side of the same kernels (ncu --set full, one launch each of an
-# 8-render batch, summarised in the profiles directory): the share of issue
-# slots used (sm__inst_issued over the schedulers' cycles) and the share of
-# a warp's 32 lanes active per instruction.  The plane and triangle tests are
-# dependent IEEE-exact FP32 chains, so these kernels are bound by issue and
-# latency rather than by DRAM.
-# Warp instructions per unit (smsp__inst_executed.sum over every launch of
-# one 8-render step, divided by that step's rays / shadow rays), for the
-# issue-rate roofline below.
-NCU_INST_PER_UNIT = {"extend": 42.36, "shade": 54.61, "shadow": 31.57}
+# 8-render batch with the queue full): the share of issue slots used and the
+# share of a warp's 32 lanes active per instruction.  The plane and triangle
+# tests are dependent IEEE-exact FP32 chains, so these kernels are bound by
+# issue and latency rather than by DRAM.
+NCU_ISSUE = {"extend": {"issue_slots_busy": 0.640, "lanes_active": 16.2 / 32},
+             "shade": {"issue_slots_busy": 0.330, "lanes_active": 23.1 / 32},
+             "shadow": {"issue_slots_busy": 0.466, "lanes_active": 21.8 / 32, "l1_busy": 0.817}}
 # Algorithmic BVH-fetch bytes per ray of the batched-mesh workload's two
 # scenes: 2 x 24 B of child boxes per internal node processed plus 36 B per
 # leaf triangle tested, counted by the reference's own traversal order
@@ -70,9 +72,6 @@ BVH_BYTES_PER_RAY = {"ico59-diffuse": 223.6, "ico59-glass": 1138.9}
 # projections onto the quad's edges); the reference tests every plane of the
 # scene for every ray, light planes included (code/Renderer.cpp:891-949).
 PLANE_TEST_FLOPS = 25
-NCU_ISSUE = {"extend": {"issue_slots_busy": 0.658, "lanes_active": 15.5 / 32},
-             "shade": {"issue_slots_busy": 0.324, "lanes_active": 23.1 / 32},
-             "shadow": {"issue_slots_busy": 0.480, "lanes_active": 21.8 / 32, "l1_busy": 0.81}}
 
 
 def args_():
@@ -648,13 +647,25 @@ def main():
         achieved = bytes_stage[dom] / (t_ms / 1e3) / 1e9
         units = ps["shadow_rays"] if dom == "shadow" else ps["rays"]
         traffic = NCU_DRAM_PER_UNIT[dom] * units / n_l if dom in NCU_DRAM_PER_UNIT else None
+        # every wavefront kernel against the same bound, for the full picture
+        per_kernel = {}
+        for k in bytes_stage:
+            if ps["stage_ms"][k] <= 0:
+                continue
+            nk = max(1, ps["stage_launches"][k])
+            gbs = bytes_stage[k] / (ps["stage_ms"][k] / 1e3) / 1e9
+            uk = ps["shadow_rays"] if k == "shadow" else ps["rays"]
+            per_kernel[f"k_{k}"] = {"ms": ps["stage_ms"][k], "achieved_gbs": gbs, "frac_hbm": gbs / peak,
+                                    "ncu_traffic_per_launch": NCU_DRAM_PER_UNIT[k] * uk / nk,
+                                    "algorithmic_bytes_per_launch": bytes_stage[k] / nk}
         roofline = {"bound": "hbm", "kernel": f"k_{dom}", "achieved": achieved, "peak": peak, "unit": "GB/s",
                     "frac": achieved / peak, "peak_kind": kind, "traffic": traffic,
                     "traffic_note": "ncu DRAM bytes per unit (8-render capture) x units per launch",
                     "bytes_per_launch": bytes_stage[dom] / n_l, "ms_per_launch": t_ms / n_l,
                     "issue": dict(NCU_ISSUE.get(dom, {}), note="ncu, one launch per kernel of an 8-render batch"),
                     "stage_ms": ps["stage_ms"], "stage_share": {k: v / max(1e-9, sum(ps["stage_ms"].values()))
-                                                                for k, v in ps["stage_ms"].items()}}
+                                                                for k, v in ps["stage_ms"].items()},
+                    "per_kernel": per_kernel}
         # The bound that applies: instruction issue.  The same kernel's warp
         # instructions (ncu per unit x units) over its CUDA-event time,
         # against one warp instruction per cycle per scheduler (4 per SM) at

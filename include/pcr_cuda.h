@@ -252,11 +252,13 @@ pcr_status pcr_engine_stats_get(pcr_ctx *ctx, pcr_engine_stats *out);
  * reference counterpart (measurement only). */
 pcr_status pcr_l2_bandwidth(pcr_ctx *ctx, int64_t bytes, int32_t reps, double *gbs);
 pcr_status pcr_engine_stats_reset(pcr_ctx *ctx);
-/* Picks queue capacity (512K..4M paths in flight), block size, chunk and
+/* Picks queue capacity (512K..16M paths in flight), block size, chunk and
  * refill cadence by timing short trial batches of the given requests; stores
  * the choice (and the cache file when one was given).  The path and shadow
- * queues grow with the capacity: about 10 GB at 4M with up to 8 shadow rays
- * per hit, more when requests ask for more (S slots per path slot). */
+ * queues grow with the capacity: about 10 GB at 4M and 40 GB at 16M with up
+ * to 8 shadow rays per hit, more when requests ask for more (S slots per
+ * path slot); capacities whose path slots times the sample's shadow rays per
+ * hit reach 2^31 shadow records are not tried. */
 pcr_status pcr_autotune(pcr_ctx *ctx, const pcr_scene_id *scenes, const pcr_render_desc *descs,
                         int32_t n, int32_t *chosen /* 4 ints, may be NULL */);
 
