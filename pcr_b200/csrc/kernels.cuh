@@ -860,24 +860,29 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kShadowMinBlocks) k_shadow(Eng
     Counters* C = E.cnt;
     const int n = min(C->shadow_n, E.shadow_cap);
     const ShadowQueue SQ = E.sq;
-    unsigned long long mine = 0;
+    unsigned mine = 0;  // shadow rays of this thread (one launch: < 2^32)
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int nx = i + gridDim.x * blockDim.x;
         if (nx < n) { prefetch_l2(SQ.o + nx); prefetch_l2(SQ.d + nx); prefetch_l2(SQ.c + nx); }
         const float4 o = SQ.o[i];
         if (!(o.w >= 0.f)) continue;  // skip record (zero geometry term)
-        const float4 d = SQ.d[i], c = SQ.c[i];
-        const int tag = __float_as_int(c.w);
-        const DScene& S = E.scenes[tag >> 16];
+        const float4 d = SQ.d[i];
+        // only the scene is needed for the query; the contribution is read
+        // afterwards, for lit samples, so it holds no registers across it
+        const DScene& S = E.scenes[__float_as_int(SQ.c[i].w) >> 16];
         const float d2 = o.w;
         // a hit beyond the light cannot block: bound the query just past it
         const float tmax = sqrtf(d2) * 1.0001f + 1e-4f;
         mine++;
-        if (!scene_blocked(S, E.mats, xyz(o), xyz(d), tmax, (double)d2 - 1e-3))
-            add_xyz(E.reqs[tag & 0xFFFF].accum + (size_t)__float_as_int(d.w) * 3, make_float3(c.x, c.y, c.z));
+        if (!scene_blocked(S, E.mats, xyz(o), xyz(d), tmax, (double)d2 - 1e-3)) {
+            const float4 c = SQ.c[i];
+            const int pixel = __float_as_int(SQ.d[i].w);
+            add_xyz(E.reqs[__float_as_int(c.w) & 0xFFFF].accum + (size_t)pixel * 3, make_float3(c.x, c.y, c.z));
+        }
     }
-    for (int off = 16; off > 0; off >>= 1) mine += __shfl_down_sync(0xffffffffu, mine, off);
-    if ((threadIdx.x & 31) == 0 && mine) atomicAdd(&C->shadow_rays, mine);
+    unsigned long long warp_rays = mine;
+    for (int off = 16; off > 0; off >>= 1) warp_rays += __shfl_down_sync(0xffffffffu, warp_rays, off);
+    if ((threadIdx.x & 31) == 0 && warp_rays) atomicAdd(&C->shadow_rays, warp_rays);
 }
 
 // ------------------------------------------------------------------ status
