@@ -6,8 +6,8 @@ Cornell scene variants, square resolutions log-uniform in 128..1024, depth
 2..8, paths per pixel log-uniform in 1..64, shadow rays 1..8, spectral
 hero-4, FP32 -- rendered by the batched method (one persistent wavefront
 over all 64 requests, graph-captured iterations).  Synthetic seeded data;
-the cornell-bunny variant uses a displaced icosphere of the bunny's size
-when the Stanford bunny OBJ is not present.
+the cornell-bunny variant renders the reference's Stanford bunny (a
+committed fixture).
 
 Printed (rank 0, one JSON line):
   value        batched paths/s (device time, CUDA events on the engine stream,
@@ -17,9 +17,17 @@ Printed (rank 0, one JSON line):
                host and copies every HDR + 8-bit image back into the caller's
                buffers as each finishes, host clock
   plain_value  the plain per-request method (one render per launch sequence)
-  roofline     dominant wavefront kernel vs measured HBM bandwidth
+  roofline     dominant wavefront kernel vs measured HBM bandwidth (all three
+               in roofline.per_kernel); roofline.bvh_fetch: the mesh leg's
+               reference-order BVH-fetch bytes vs measured HBM and L2;
+               roofline.fp32_issue: Cornell's plane-test flops vs FP32 peak
   cpu_baseline the reference CPU renderer (oracle/_ref, built from the
                reference sources) on a bounded row sample of the same batch
+  mesh_batch   batched mesh scenes (32 renders on the ~70k-triangle mesh)
+  serve, serve_scale
+               served streams with p50 / p99 latency (Poisson arrivals;
+               the at-scale stream mixes heavy 2048^2 renders on a
+               1M-triangle mesh with small ones)
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 """
@@ -730,13 +738,13 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": a.steps,
             "warmup": a.warmup, "ms_per_step": ms / a.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic: seeded 64-render batch of the 10 Cornell variants (bunny -> displaced icosphere "
-                    "stand-in when its OBJ is absent)",
+            "data": "synthetic: seeded 64-render batch of the 10 Cornell variants (cornell-bunny with the "
+                    "reference's Stanford bunny, a committed fixture)",
             "config": {"workload": f"batch{a.renders}-uneven", "renders": a.renders, "paths_per_step": step_paths,
                        "parallelism": f"replicas x{world} (own seeded batch per GPU, no collective)",
                        "resolution": "square, log-uniform 128..1024", "depth": "2..8", "paths_per_pixel": "1..64",
                        "shadow_rays": "1..8", "spectral": "hero-4",
-                       "l2": "path/shadow queues (2-10 GB at the tuned 1M-4M paths in flight) > 126 MB L2 (no flush needed)"},
+                       "l2": "path/shadow queues (2-40 GB at the tuned 1M-16M paths in flight) > 126 MB L2 (no flush needed)"},
             "rays_per_s": rays,
             "work": {"paths": step_paths * a.steps, "rays": st["rays"], "shadow_rays": st["shadow_rays"],
                      "iterations": st.get("iterations")},

@@ -10,9 +10,10 @@
   paths per pixel, shadow rays) drawn by seed.
 * request_stream(...): Poisson arrivals for the served method.
 
-The Stanford bunny OBJ is not shipped with this package; where a workload
-draws the cornell-bunny variant and the OBJ is absent, a displaced icosphere
-of the bunny's triangle count stands in for it (same pose and material).
+The Stanford bunny OBJ is a test fixture of this repository
+(tests/golden/models); where a workload draws the cornell-bunny variant and
+that file is absent, a displaced icosphere of the bunny's triangle count
+stands in for it (same pose and material).
 """
 from __future__ import annotations
 
