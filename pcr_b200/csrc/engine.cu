@@ -120,6 +120,7 @@ Engine::Engine(const pcr_ctx_opts* o)
     CK(cudaSetDevice(device_));
     CK(cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, device_));
     CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&resolve_stream_, cudaStreamNonBlocking));
     xyz_scale_ = (700.f - 400.f) / host_ybar_integral();
     slot_owner_.assign(kMaxActive, -1);
     scenes_.reserve(256);
@@ -146,6 +147,7 @@ Engine::~Engine()
     }
     cudaSetDevice(device_);
     cudaStreamSynchronize(stream_);
+    cudaStreamSynchronize(resolve_stream_);
     for (auto& kv : reqs_) {
         Request& r = *kv.second;
         if (r.accum) cudaFreeAsync(r.accum, stream_);
@@ -157,6 +159,7 @@ Engine::~Engine()
         if (r.ev_ready) cudaEventDestroy(r.ev_ready);
     }
     cudaStreamSynchronize(stream_);
+    cudaStreamDestroy(resolve_stream_);
     for (Staging& st : staging_idle_) {
         cudaStreamSynchronize(st.stream);
         if (st.buf) cudaFreeHost(st.buf);
@@ -953,31 +956,39 @@ void Engine::check_status()
                                                   std::to_string(h_snap_->cnt.status) + ")");
 }
 
-void Engine::finish_request(Request& r)
+void Engine::finish_request(Request& r, bool after_engine_stream)
 {
     const pcr_render_desc& d = r.desc;
     const int64_t px = (int64_t)d.width * d.height;
     // adaptive requests hold each pixel's final mean already
     const double inv = adaptive_rounds(d) ? 1.0 : 1.0 / ((double)d.samples * std::max(1, d.aa_samples));
     int grid = std::min<int64_t>((px + 255) / 256, (int64_t)sms_ * 8);
-    k_resolve<<<std::max(1, grid), 256, 0, stream_>>>(r.accum, (int)px, inv, d.spectral ? 1 : 0, d.aces ? 1 : 0,
-                                                       r.d_hdr, r.d_rgb);
+    cudaStream_t rs = resolve_stream_;
+    if (after_engine_stream) {
+        // the plain method hands over with work it queued since its last
+        // synchronisation: the resolve follows all of it
+        if (!r.ev_ready) CK(cudaEventCreateWithFlags(&r.ev_ready, cudaEventDisableTiming));
+        CK(cudaEventRecord(r.ev_ready, stream_));
+        CK(cudaStreamWaitEvent(rs, r.ev_ready, 0));
+    }
+    k_resolve<<<std::max(1, grid), 256, 0, rs>>>(r.accum, (int)px, inv, d.spectral ? 1 : 0, d.aces ? 1 : 0, r.d_hdr,
+                                                 r.d_rgb);
     CK(cudaGetLastError());
     if (d.denoise) {
         // two bilateral passes on the 8-bit image, the accumulator as scratch
         unsigned char* tmp = reinterpret_cast<unsigned char*>(r.accum);
-        k_bilateral<<<std::max(1, grid), 256, 0, stream_>>>(r.d_rgb, tmp, d.width, d.height);
-        k_bilateral<<<std::max(1, grid), 256, 0, stream_>>>(tmp, r.d_rgb, d.width, d.height);
+        k_bilateral<<<std::max(1, grid), 256, 0, rs>>>(r.d_rgb, tmp, d.width, d.height);
+        k_bilateral<<<std::max(1, grid), 256, 0, rs>>>(tmp, r.d_rgb, d.width, d.height);
         CK(cudaGetLastError());
     }
     // the resolved images stay on the device until fetch copies them out
-    CK(cudaFreeAsync(r.accum, stream_));
+    CK(cudaFreeAsync(r.accum, rs));
     r.accum = nullptr;
     for (int k = 0; k < 2; k++)
-        if (r.act[k]) { CK(cudaFreeAsync(r.act[k], stream_)); r.act[k] = nullptr; }
-    if (r.welford) { CK(cudaFreeAsync(r.welford, stream_)); r.welford = nullptr; }
+        if (r.act[k]) { CK(cudaFreeAsync(r.act[k], rs)); r.act[k] = nullptr; }
+    if (r.welford) { CK(cudaFreeAsync(r.welford, rs)); r.welford = nullptr; }
     if (!r.ev_ready) CK(cudaEventCreateWithFlags(&r.ev_ready, cudaEventDisableTiming));
-    CK(cudaEventRecord(r.ev_ready, stream_));
+    CK(cudaEventRecord(r.ev_ready, rs));
     r.state = ReqState::Resolving;
 }
 
@@ -1119,6 +1130,7 @@ bool Engine::engine_step()
         if (active_slots_.empty()) {
             if (resolving || snap_inflight_) {
                 CK(cudaStreamSynchronize(stream_));
+                CK(cudaStreamSynchronize(resolve_stream_));
                 if (snap_inflight_) {
                     const int last = (snap_next_ + kSnapRing - 1) % kSnapRing;
                     h_snap_ = h_snaps_[last];
@@ -1181,6 +1193,7 @@ void Engine::run_until_idle()
         last_paths = h_snap_->cnt.paths;
     }
     CK(cudaStreamSynchronize(stream_));
+    CK(cudaStreamSynchronize(resolve_stream_));
     std::lock_guard<std::mutex> l(mu_);
     harvest(true);
 }
@@ -1262,6 +1275,7 @@ void Engine::wait(int64_t id, int64_t timeout_ms)
             std::lock_guard<std::mutex> g(run_mu_);
             if (!engine_step()) {
                 CK(cudaStreamSynchronize(stream_));
+                CK(cudaStreamSynchronize(resolve_stream_));
                 std::lock_guard<std::mutex> l(mu_);
                 harvest(true);
             }
@@ -1412,7 +1426,7 @@ void Engine::render_plain(int scene, const pcr_render_desc& desc, float* hdr, ui
     unsigned long long tf = 0, td = 0;
     CK(cudaMemcpy(&tf, d_tfirst_, 8, cudaMemcpyDeviceToHost));
     CK(cudaMemcpy(&td, d_tdone_, 8, cudaMemcpyDeviceToHost));
-    finish_request(r);
+    finish_request(r, true);
     active_slots_.clear();
     active_dirty_ = true;
     bytes_in_use_ -= r.bytes;

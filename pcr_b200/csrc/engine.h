@@ -120,7 +120,7 @@ private:
     void launch_block();
     void build_graph();
     void harvest(bool final_sync);
-    void finish_request(Request& r);
+    void finish_request(Request& r, bool after_engine_stream = false);
     void release_cancelled(Request& r);
     void copy_out(Request& r, float* hdr, uint8_t* rgb);
     DRequest make_request(const pcr_render_desc& d, int scene, double* accum) const;
@@ -133,6 +133,10 @@ private:
     int device_ = 0;
     int sms_ = 148;
     cudaStream_t stream_ = nullptr;
+    // Resolves of finished requests run here, beside the iterations still
+    // queued on stream_: a request is harvested from the device state copied
+    // after the block it finished in, by which point its accumulator is final.
+    cudaStream_t resolve_stream_ = nullptr;
     // Result copies: pinned staging buffers, each with its own copy stream,
     // kept idle between fetches.  A fetch takes one (or makes one), so
     // fetches from several threads copy at the same time.
