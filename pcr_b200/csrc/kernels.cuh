@@ -501,6 +501,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
         // rarely straddle two blocks' records, which may belong to
         // different scenes.
         int nee = 0;
+        bool mesh = false;  // casts over a BVH
         if (live && (prim & kPrimKindMask) != kPrimNone) {
             const DScene& S0 = E.scenes[id.w];
             if (S0.total_light_area > 0.f) {
@@ -508,11 +509,13 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                 const int mi0 = k0 == kPrimSphere ? S0.spheres[p0].mat.x
                               : k0 == kPrimPlane  ? __float_as_int(S0.planes[p0].o_mat.w)
                                                   : __float_as_int(S0.tris[p0].e1_mat.w);
-                if (!(M[S0.mat_base + mi0].flags & (kMatEmissive | kMatMetallic | kMatTransparent)))
+                if (!(M[S0.mat_base + mi0].flags & (kMatEmissive | kMatMetallic | kMatTransparent))) {
                     nee = E.reqs[slot].shadow;
+                    mesh = S0.n_nodes > 0;
+                }
             }
         }
-        int spos_block;
+        int spos_block, sstride;
         {
             int ex = nee;  // inclusive scan across the warp
 #pragma unroll
@@ -530,7 +533,24 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                 sw[kShadeBlock / 32] = tot ? atomicAdd(&C->shadow_n, tot) : 0;
             }
             __syncthreads();
-            spos_block = sw[kShadeBlock / 32] + sw[wid] + ex - nee;
+            const int wbase = sw[kShadeBlock / 32] + sw[wid];
+            // Sample-major order inside the warp when its vertices all cast
+            // the same number of shadow rays (one request, the usual case)
+            // into scenes without a mesh: record s of the warp's k-th
+            // casting lane sits at wbase + s * casters + k, so each sample's
+            // stores are one contiguous run.  Otherwise each lane's records
+            // are adjacent: over a BVH, the rays of one vertex then share a
+            // k_shadow warp and walk mostly the same nodes.
+            const unsigned cm = __ballot_sync(0xffffffffu, nee > 0);
+            const unsigned hi = __reduce_max_sync(0xffffffffu, (unsigned)nee);
+            const unsigned lo = __reduce_min_sync(0xffffffffu, nee > 0 ? (unsigned)nee : 0xffffffffu);
+            if (hi == lo && !__any_sync(0xffffffffu, mesh)) {
+                spos_block = wbase + __popc(cm & ((1u << lane) - 1u));
+                sstride = __popc(cm);
+            } else {
+                spos_block = wbase + ex - nee;
+                sstride = 1;
+            }
         }
 
         if (live && (prim & kPrimKindMask) != kPrimNone) {
@@ -705,7 +725,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         cached = S.emit_mat;
                     }
                     const int spos = spos_block;
-                    const int nsh = spos + R.shadow <= E.shadow_cap ? R.shadow : 0;
+                    const int nsh = spos + (R.shadow - 1) * sstride < E.shadow_cap ? R.shadow : 0;
                     if (nsh == 0) atomicOr(&C->status, 1);
                     for (int s = 0; s < nsh; s++) {
                         const float4 rr = rand4(R, (uint32_t)id.y, (uint32_t)id.z, (uint32_t)fork, (uint32_t)bounce,
@@ -756,7 +776,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
                         else { hc = f3add(hc, f3mul(N, 1e-3f)); so = hc; }
                         const float cosL = fmaxf(0.f, -f3dot(Nl, Li));
                         const float G = cosT * cosL * (inv_d * inv_d);
-                        const int pos = spos + s;
+                        const int pos = spos + s * sstride;
                         if (!(G > 0.f)) {
                             SQ.o[pos] = make_float4(0.f, 0.f, 0.f, -1.f);  // skip record
                             continue;
