@@ -402,11 +402,17 @@ __global__ void __launch_bounds__(kTraceMaxBlock, kTraceMinBlocks) k_extend(Engi
 
 // ------------------------------------------------------------------ helpers
 
+// Adds one sample's XYZ to a pixel's FP64 accumulator (device memory) with
+// global-space reductions, which return nothing to the thread.
+__device__ __forceinline__ void red_add(double* a, double v)
+{
+    asm volatile("red.global.add.f64 [%0], %1;" ::"l"(__cvta_generic_to_global(a)), "d"(v) : "memory");
+}
 __device__ __forceinline__ void add_xyz(double* acc, float3 c)
 {
-    atomicAdd(acc + 0, (double)c.x);
-    atomicAdd(acc + 1, (double)c.y);
-    atomicAdd(acc + 2, (double)c.z);
+    red_add(acc + 0, (double)c.x);
+    red_add(acc + 1, (double)c.y);
+    red_add(acc + 2, (double)c.z);
 }
 
 // ------------------------------------------------------------------ shade
