@@ -485,6 +485,7 @@ __global__ void __launch_bounds__(kShadeBlock, PCR_SHADE_MIN_BLOCKS) k_shade(Eng
             const int nx = i + stride;
             prefetch_l2(Q.id + nx); prefetch_l2(Q.o + nx); prefetch_l2(Q.d + nx); prefetch_l2(Q.tp + nx);
             prefetch_l2(E.hit + nx);
+            prefetch_l2(Q.w[0] + nx); prefetch_l2(Q.w[1] + nx); prefetch_l2(Q.w[2] + nx);
         }
         if (live) { id = Q.id[i]; o4 = Q.o[i]; d4 = Q.d[i]; tp4 = Q.tp[i]; h = E.hit[i]; }
         const int slot = id.x;
