@@ -55,18 +55,18 @@ HBM_FALLBACK = 6650.0
 # replayed alone with a cold L2; the summary and command are kept in the
 # profiles directory).  Traffic grows in proportion to the units, so a
 # launch's traffic is this figure times its units.
-NCU_DRAM_PER_UNIT = {"extend": 61.0, "shade": 535.1, "shadow": 83.2}
+NCU_DRAM_PER_UNIT = {"extend": 61.0, "shade": 548.7, "shadow": 83.2}
 # Warp instructions per unit (smsp__inst_executed.sum over the same
 # launches, divided by the same units), for the issue-rate roofline below.
-NCU_INST_PER_UNIT = {"extend": 48.22, "shade": 69.70, "shadow": 43.89}
+NCU_INST_PER_UNIT = {"extend": 48.25, "shade": 69.57, "shadow": 43.90}
 # Issue-rate side of the same kernels (ncu --set full, one launch each of an
 # 8-render batch with the queue full): the share of issue slots used and the
 # share of a warp's 32 lanes active per instruction.  The plane and triangle
 # tests are dependent IEEE-exact FP32 chains, so these kernels are bound by
 # issue and latency rather than by DRAM.
-NCU_ISSUE = {"extend": {"issue_slots_busy": 0.644, "lanes_active": 16.2 / 32},
-             "shade": {"issue_slots_busy": 0.374, "lanes_active": 23.2 / 32},
-             "shadow": {"issue_slots_busy": 0.572, "lanes_active": 17.6 / 32, "l1_busy": 0.648}}
+NCU_ISSUE = {"extend": {"issue_slots_busy": 0.638, "lanes_active": 16.2 / 32},
+             "shade": {"issue_slots_busy": 0.382, "lanes_active": 23.2 / 32},
+             "shadow": {"issue_slots_busy": 0.573, "lanes_active": 17.6 / 32, "l1_busy": 0.649}}
 # Algorithmic BVH-fetch bytes per ray of the batched-mesh workload's two
 # scenes: 2 x 24 B of child boxes per internal node processed plus 36 B per
 # leaf triangle tested, counted by the reference's own traversal order
